@@ -1,0 +1,338 @@
+"""Benchmark: Richardson-Lucy (Clarity_MaximumLikelihoodDeconvolve) on a
+256x256x64 fp32 volume with a same-size PSF (work box 512x512x128), 200
+iterations per step -- the RL leg of the 256x256x64 plain-methods workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is whole-job throughput in image
+voxel-iterations per second (G) with inputs resident in HBM, timed with CUDA
+events on the launching stream, max over ranks; `e2e` is the same metric
+through the public C API with host buffers (pinned), copies included.
+Multi-GPU runs are independent replicas (one volume per GPU, no collective
+on the data path); `value` sums the ranks' work over the slowest rank's time.
+
+`--impl reference` times the reference's own CPU implementation (the
+unmodified reference sources built into oracle/_ref with the project's
+FFTW-API shim) on a bounded sample of the same workload, on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RL Gvoxel-iter/s @256²×64 fp32"
+UNIT = "Gvoxel-iter/s"
+IMAGE_ZYX = (64, 256, 256)
+ITERS = 200
+WORKLOAD = "Richardson-Lucy (MaximumLikelihoodDeconvolve) 256x256x64 fp32, same-size PSF " \
+           "(0.9 G(2,5) + 0.1 G(6,12)), 200 iterations per step"
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for ln in f:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# --------------------------------------------------------------- CPU legs
+def cpu_reference_rl(img, psf, iters):
+    """Reference CPU code (oracle/_ref) or, where it was not built, the
+    oracle restatement; returns (seconds, kind, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    if O.ReferenceCPU.available("ref"):
+        ref = O.ReferenceCPU("ref")
+        ref.set_threads(cores)
+        t0 = time.perf_counter()
+        ref.rl(img, psf, iters)
+        return time.perf_counter() - t0, "reference", cores
+    orc = O.Oracle()
+    orc.set_threads(cores)
+    t0 = time.perf_counter()
+    orc.rl(img, psf, iters)
+    return time.perf_counter() - t0, "port", cores
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from clarity_b200 import synthetic as syn
+    img, psf, _ = syn.cfg1(seed=1)
+    iters_per_step = 1
+    for _ in range(args.warmup):
+        cpu_reference_rl(img, psf, iters_per_step)
+    times = []
+    kind = cores = None
+    for _ in range(args.steps):
+        t, kind, cores = cpu_reference_rl(img, psf, iters_per_step)
+        times.append(t)
+    ms = 1e3 * sum(times) / len(times)
+    vox = int(np.prod(IMAGE_ZYX))
+    value = vox * iters_per_step / (ms / 1e3) / 1e9
+    sample = f"RL on the 256x256x64 workload, {iters_per_step} iteration per step (work box " \
+             f"512x512x128), all {cores} host threads"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD.replace("200 iterations", f"{iters_per_step} iteration"),
+                       "image_xyz": [256, 256, 64], "psf_xyz": [256, 256, 64],
+                       "iterations_per_step": iters_per_step, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+def family_bytes(work, img_vox, ker_vox, iters):
+    """Algorithmic HBM bytes of one RL solve, per kernel family.
+    C = complex half spectrum 8*nz*ny*(nx/2+1); R = real work box 4*N;
+    image/kernel are read unpadded (4 bytes per voxel)."""
+    nz, ny, nx = work
+    N = nx * ny * nz
+    C = 8 * nz * ny * (nx // 2 + 1)
+    R = 4 * N
+    Ri, Rk = 4 * img_vox, 4 * ker_vox
+    return {
+        "xy_forward": (Rk + C) + (Ri + C) + (iters - 1) * (R + C),
+        "z": 2 * C + 2 * iters * 3 * C,
+        "xy_inv_fwd": iters * (2 * C + Ri),
+        "xy_inverse": (C + Ri + R) + (iters - 1) * (C + 2 * R),
+        "per_iteration_survey": 4 * R + 10 * C,
+    }
+
+
+def run_gpu_arm(args, rank, world):
+    import torch
+    from clarity_b200 import api, synthetic as syn
+
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    api.set_device(local)
+    api.register()
+    img, psf, _ = syn.cfg1(seed=1 + rank)
+    img_d = torch.from_numpy(img).cuda()
+    psf_d = torch.from_numpy(psf).cuda()
+    out_d = torch.empty_like(img_d)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        api.ml_device(img_d, psf_d, out_d, ITERS, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    api.timing_enable(True)
+    l0 = api.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = api.launch_count() - l0
+    fam = api.timing_collect()
+    api.timing_enable(False)
+    ms_total = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+        dist.barrier()
+    ms_step = ms_total / args.steps
+    vox = int(np.prod(IMAGE_ZYX))
+    value = world * vox * ITERS / (ms_step / 1e3) / 1e9
+
+    # end to end through the public C API with pinned host buffers
+    img_h = torch.empty(IMAGE_ZYX, dtype=torch.float32, pin_memory=True).numpy()
+    psf_h = torch.empty(IMAGE_ZYX, dtype=torch.float32, pin_memory=True).numpy()
+    img_h[...] = img
+    psf_h[...] = psf
+    out_h = torch.empty(IMAGE_ZYX, dtype=torch.float32, pin_memory=True).numpy()
+    lib = api.load()
+
+    def e2e_step():
+        rc = lib.Clarity_MaximumLikelihoodDeconvolve(img_h, api.dim3(img_h), psf_h,
+                                                     api.dim3(psf_h), out_h, ITERS)
+        api._check(rc)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    clk = clocks.stop()
+    e2e_value = world * vox * ITERS / (e2e_ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel family
+    work = tuple(2 * s for s in IMAGE_ZYX)
+    fb = family_bytes(work, vox, vox, ITERS)
+    peak, peak_kind = peaks()
+    fam_ms = {k: v for k, v in fam.items() if k != "other" and v[1] > 0}
+    dom = max(fam_ms, key=lambda k: fam_ms[k][0]) if fam_ms else None
+    roof = None
+    if dom:
+        tot_ms, cnt = fam_ms[dom]
+        per_launch_ms = tot_ms / cnt
+        bytes_per_launch = fb[dom] / (cnt / args.steps)
+        achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "bytes_per_launch": bytes_per_launch,
+                "ms_per_launch": per_launch_ms,
+                "share_of_step": tot_ms / ms_total}
+    iter_bytes = fb["per_iteration_survey"]
+    iter_ms = ms_step / ITERS
+    families = {k: {"ms_per_launch": v[0] / v[1], "launches_per_step": v[1] / args.steps,
+                    "GBps": (fb[k] / (v[1] / args.steps)) / (v[0] / v[1] / 1e3) / 1e9}
+                for k, v in fam_ms.items()}
+
+    if rank == 0:
+        sample_iters = max(1, args.cpu_iters)
+        t_cpu, kind, cores = cpu_reference_rl(img, psf, sample_iters)
+        cpu_value = vox * sample_iters / t_cpu / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded phantom, Poisson noise)",
+            "config": {"workload": WORKLOAD, "image_xyz": [256, 256, 64],
+                       "psf_xyz": [256, 256, 64], "work_box_xyz": [512, 512, 128],
+                       "iterations_per_step": ITERS, "parallelism": f"replicas x{world}",
+                       "l2": "inputs and working set (~0.7 GB) larger than L2"},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(img_h.nbytes + psf_h.nbytes),
+                    "d2h_bytes_per_step": int(out_h.nbytes), "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "iteration": {"ms": iter_ms, "algorithmic_bytes": iter_bytes,
+                          "GBps": iter_bytes / (iter_ms / 1e3) / 1e9,
+                          "frac": iter_bytes / (iter_ms / 1e3) / 1e9 / peak},
+            "families": families,
+            "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": cores,
+                             "kind": kind,
+                             "sample": f"RL on the same 256x256x64 workload, {sample_iters} "
+                                       f"iteration(s), {cores} host threads"},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    api.unregister()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-iters", type=int, default=4)
+    args = ap.parse_args()
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_gpu_arm(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

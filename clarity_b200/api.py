@@ -1,0 +1,340 @@
+"""Python mirror of the Clarity C API over the in-tree libclarity.so.
+
+The function names, argument meaning and result codes follow the reference
+header (Clarity.h.in:88-383): ``Clarity_MaximumLikelihoodDeconvolve(inImage,
+imageDim, kernelImage, kernelDim, outImage, iterations)`` becomes
+``maximum_likelihood_deconvolve(image, kernel, iterations)`` on numpy arrays in
+(z, y, x) order (x fastest, the reference's memory layout), returning a new
+array.  Every call goes through the C ABI; a non-success code raises
+:class:`ClarityError` carrying the code and the library's message.
+
+The ``*_device`` variants take torch CUDA tensors and run on the given (or
+current) torch stream without host copies.
+
+There is no CPU fallback: loading fails loudly if libclarity.so is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libclarity.so")
+
+# ClarityResult_t (Clarity.h.in:90-101); the numeric order is ABI.
+CLARITY_FFT_FAILED = 0
+CLARITY_OUT_OF_MEMORY = 1
+CLARITY_DEVICE_OUT_OF_MEMORY = 2
+CLARITY_INVALID_OPERATION = 3
+CLARITY_INVALID_ARGUMENT = 4
+CLARITY_SUCCESS = 5
+
+RESULT_NAMES = {
+    0: "CLARITY_FFT_FAILED", 1: "CLARITY_OUT_OF_MEMORY",
+    2: "CLARITY_DEVICE_OUT_OF_MEMORY", 3: "CLARITY_INVALID_OPERATION",
+    4: "CLARITY_INVALID_ARGUMENT", 5: "CLARITY_SUCCESS",
+}
+
+# Every symbol include/clarity.h and include/clarity_ext.h declare.
+PUBLIC_SYMBOLS = [
+    "Clarity_Dim3FromArray", "Clarity_Register", "Clarity_UnRegister",
+    "Clarity_SetNumberOfThreads", "Clarity_ImagePadSpatialShift", "Clarity_ImageClip",
+    "Clarity_ResultString", "Clarity_WienerDeconvolve",
+    "Clarity_JansenVanCittertDeconvolve", "Clarity_SmoothedJansenVanCittertDeconvolve",
+    "Clarity_IDivergenceDeconvolve", "Clarity_MaximumLikelihoodDeconvolve",
+    "Clarity_BlindMaximumLikelihoodDeconvolve", "Clarity_Convolve",
+]
+EXTENSION_SYMBOLS = [
+    "clarityx_last_error", "clarityx_set_device", "clarityx_inject_device_alloc_failure",
+    "clarityx_trim", "clarityx_synchronize", "clarityx_convolve_device",
+    "clarityx_wiener_device", "clarityx_ml_device", "clarityx_blind_ml_device",
+    "clarityx_jvc_device", "clarityx_idivergence", "clarityx_plan_info",
+    "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
+]
+
+
+class ClarityError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        self.code = code
+        super().__init__(f"{RESULT_NAMES.get(code, code)}: {message}")
+
+
+class Dim3(C.Structure):
+    """Clarity_Dim3 (Clarity.h.in:110-114)."""
+    _fields_ = [("x", C.c_int), ("y", C.c_int), ("z", C.c_int)]
+
+    def __repr__(self) -> str:
+        return f"Dim3({self.x}, {self.y}, {self.z})"
+
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libclarity.so (raises if it has not been built)."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                f"{path} is missing: build it with `python -m clarity_b200.build`")
+        L = C.CDLL(path)
+        i, u, f, vp = C.c_int, C.c_uint, C.c_float, C.c_void_p
+        L.Clarity_Dim3FromArray.argtypes = [C.POINTER(C.c_int)]
+        L.Clarity_Dim3FromArray.restype = Dim3
+        L.Clarity_Register.restype = i
+        L.Clarity_UnRegister.restype = i
+        L.Clarity_SetNumberOfThreads.argtypes = [u]
+        L.Clarity_SetNumberOfThreads.restype = i
+        L.Clarity_ImagePadSpatialShift.argtypes = [_f32p, Dim3, _f32p, Dim3,
+                                                   C.POINTER(C.c_int), f]
+        L.Clarity_ImagePadSpatialShift.restype = i
+        L.Clarity_ImageClip.argtypes = [_f32p, Dim3, _f32p, Dim3]
+        L.Clarity_ImageClip.restype = i
+        L.Clarity_ResultString.argtypes = [i]
+        L.Clarity_ResultString.restype = C.c_char_p
+        for name, extra in [("Clarity_WienerDeconvolve", [f]),
+                            ("Clarity_JansenVanCittertDeconvolve", [i]),
+                            ("Clarity_MaximumLikelihoodDeconvolve", [i]),
+                            ("Clarity_BlindMaximumLikelihoodDeconvolve", [i]),
+                            ("Clarity_Convolve", []),
+                            ("Clarity_IDivergenceDeconvolve", [])]:
+            fn = getattr(L, name)
+            fn.argtypes = [_f32p, Dim3, _f32p, Dim3, _f32p] + extra
+            fn.restype = i
+        L.Clarity_SmoothedJansenVanCittertDeconvolve.argtypes = [
+            _f32p, Dim3, _f32p, Dim3, _f32p, u, u, C.POINTER(C.POINTER(C.c_float))]
+        L.Clarity_SmoothedJansenVanCittertDeconvolve.restype = i
+        L.clarityx_last_error.restype = C.c_char_p
+        L.clarityx_set_device.argtypes = [i]
+        L.clarityx_set_device.restype = i
+        L.clarityx_inject_device_alloc_failure.argtypes = [i]
+        L.clarityx_inject_device_alloc_failure.restype = None
+        L.clarityx_trim.restype = i
+        L.clarityx_synchronize.argtypes = [vp]
+        L.clarityx_synchronize.restype = i
+        for name, extra in [("clarityx_convolve_device", []),
+                            ("clarityx_wiener_device", [f]),
+                            ("clarityx_ml_device", [i]),
+                            ("clarityx_blind_ml_device", [i]),
+                            ("clarityx_jvc_device", [i])]:
+            fn = getattr(L, name)
+            fn.argtypes = [vp, Dim3, vp, Dim3, vp] + extra + [vp]
+            fn.restype = i
+        L.clarityx_idivergence.argtypes = [_f32p, _f32p, C.c_longlong,
+                                           C.POINTER(C.c_double)]
+        L.clarityx_idivergence.restype = i
+        L.clarityx_plan_info.argtypes = [Dim3, C.POINTER(C.c_int), i]
+        L.clarityx_plan_info.restype = i
+        L.clarityx_launch_count.restype = C.c_longlong
+        L.clarityx_timing_enable.argtypes = [i]
+        L.clarityx_timing_enable.restype = None
+        L.clarityx_timing_collect.argtypes = [C.POINTER(C.c_double),
+                                              C.POINTER(C.c_longlong), i]
+        L.clarityx_timing_collect.restype = None
+        _lib = L
+        return L
+
+
+def _check(code: int) -> None:
+    if code != CLARITY_SUCCESS:
+        msg = load().clarityx_last_error().decode(errors="replace")
+        raise ClarityError(code, msg)
+
+
+def dim3(a) -> Dim3:
+    """numpy (z, y, x) shape (or array) -> Clarity_Dim3(x, y, z)."""
+    shape = a.shape if hasattr(a, "shape") else tuple(a)
+    z, y, x = shape
+    return Dim3(int(x), int(y), int(z))
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# ------------------------------------------------------------ lifecycle
+def register() -> None:
+    """Clarity_Register (src/Clarity.cxx:46-79)."""
+    _check(load().Clarity_Register())
+
+
+def unregister() -> None:
+    """Clarity_UnRegister (src/Clarity.cxx:82-91)."""
+    _check(load().Clarity_UnRegister())
+
+
+def set_number_of_threads(n: int) -> None:
+    _check(load().Clarity_SetNumberOfThreads(int(n)))
+
+
+def result_string(code: int) -> str:
+    return load().Clarity_ResultString(int(code)).decode()
+
+
+def set_device(device: int) -> None:
+    _check(load().clarityx_set_device(int(device)))
+
+
+def inject_device_alloc_failure(countdown: int) -> None:
+    load().clarityx_inject_device_alloc_failure(int(countdown))
+
+
+def trim() -> None:
+    _check(load().clarityx_trim())
+
+
+# ------------------------------------------------------------- utilities
+def image_pad_spatial_shift(src, dst_shape_zyx, shift_xyz, fill=0.0) -> np.ndarray:
+    """Clarity_ImagePadSpatialShift (src/ImagePadSpatialShift.cxx:32-69)."""
+    src = _f32(src)
+    dst = np.empty(tuple(dst_shape_zyx), dtype=np.float32)
+    sh = (C.c_int * 3)(*[int(v) for v in shift_xyz])
+    _check(load().Clarity_ImagePadSpatialShift(dst, dim3(dst), src, dim3(src), sh,
+                                               float(fill)))
+    return dst
+
+
+def image_clip(src, dst_shape_zyx) -> np.ndarray:
+    """Clarity_ImageClip (src/ImageClip.cxx:30-50)."""
+    src = _f32(src)
+    dst = np.empty(tuple(dst_shape_zyx), dtype=np.float32)
+    _check(load().Clarity_ImageClip(dst, dim3(dst), src, dim3(src)))
+    return dst
+
+
+# ------------------------------------------------------------ algorithms
+def _host(name, image, kernel, *extra) -> np.ndarray:
+    image, kernel = _f32(image), _f32(kernel)
+    out = np.empty_like(image)
+    _check(getattr(load(), name)(image, dim3(image), kernel, dim3(kernel), out, *extra))
+    return out
+
+
+def convolve(image, kernel) -> np.ndarray:
+    """Clarity_Convolve (src/Convolve.cxx:41-115)."""
+    return _host("Clarity_Convolve", image, kernel)
+
+
+def wiener_deconvolve(image, kernel, epsilon: float) -> np.ndarray:
+    """Clarity_WienerDeconvolve (src/WienerDeconvolve.cxx:211-290)."""
+    return _host("Clarity_WienerDeconvolve", image, kernel, float(epsilon))
+
+
+def maximum_likelihood_deconvolve(image, kernel, iterations: int) -> np.ndarray:
+    """Clarity_MaximumLikelihoodDeconvolve (src/MaximumLikelihoodDeconvolve.cxx:255-332)."""
+    return _host("Clarity_MaximumLikelihoodDeconvolve", image, kernel, int(iterations))
+
+
+def blind_maximum_likelihood_deconvolve(image, kernel, iterations: int) -> np.ndarray:
+    """Clarity_BlindMaximumLikelihoodDeconvolve (src/BlindMaximumLikelihoodDeconvolve.cxx:249-317)."""
+    return _host("Clarity_BlindMaximumLikelihoodDeconvolve", image, kernel,
+                 int(iterations))
+
+
+def jansen_van_cittert_deconvolve(image, kernel, iterations: int) -> np.ndarray:
+    """Clarity_JansenVanCittertDeconvolve (src/JansenVanCittertDeconvolve.cxx:311-389)."""
+    return _host("Clarity_JansenVanCittertDeconvolve", image, kernel, int(iterations))
+
+
+def smoothed_jansen_van_cittert_deconvolve(image, kernel, iterations: int,
+                                           smooth_interval: int,
+                                           smooth_sigma_xyz=None) -> np.ndarray:
+    """Clarity_SmoothedJansenVanCittertDeconvolve (Clarity.h.in:285-291)."""
+    image, kernel = _f32(image), _f32(kernel)
+    out = np.empty_like(image)
+    if smooth_sigma_xyz is None:
+        arr = None
+    else:
+        vals = [C.c_float(float(s)) for s in smooth_sigma_xyz]
+        arr = (C.POINTER(C.c_float) * 3)(*[C.pointer(v) for v in vals])
+    _check(load().Clarity_SmoothedJansenVanCittertDeconvolve(
+        image, dim3(image), kernel, dim3(kernel), out, int(iterations),
+        int(smooth_interval), arr))
+    return out
+
+
+def idivergence_deconvolve(image, kernel) -> np.ndarray:
+    """Clarity_IDivergenceDeconvolve: the reference stub writes zeros."""
+    return _host("Clarity_IDivergenceDeconvolve", image, kernel)
+
+
+def idivergence(g, ghat) -> float:
+    """FP64 I-divergence sum g ln(g/ghat) + ghat - g (clarityx_idivergence)."""
+    g, ghat = _f32(g).ravel(), _f32(ghat).ravel()
+    if g.size != ghat.size:
+        raise ValueError("size mismatch")
+    r = C.c_double(0.0)
+    _check(load().clarityx_idivergence(g, ghat, g.size, C.byref(r)))
+    return float(r.value)
+
+
+def plan_info(work_shape_zyx) -> dict:
+    keys = ["M", "XS", "Ay", "By", "G", "W", "KG", "xy_blocks", "z_blocks", "xy_smem",
+            "z_smem", "x_passes", "y0_passes", "z_passes", "xmode", "spec_kelems"]
+    f = (C.c_int * 16)()
+    _check(load().clarityx_plan_info(dim3(work_shape_zyx), f, 16))
+    return dict(zip(keys, list(f)))
+
+
+# ------------------------------------------------------------ probes
+KERNEL_FAMILIES = ["xy_forward", "z", "xy_inv_fwd", "xy_inverse", "other"]
+
+
+def launch_count() -> int:
+    return int(load().clarityx_launch_count())
+
+
+def timing_enable(on: bool = True) -> None:
+    load().clarityx_timing_enable(1 if on else 0)
+
+
+def timing_collect() -> dict:
+    ms = (C.c_double * 5)()
+    cnt = (C.c_longlong * 5)()
+    load().clarityx_timing_collect(ms, cnt, 5)
+    return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_FAMILIES)}
+
+
+# ------------------------------------------------------ device variants
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _dev(name, image, kernel, out, extra, stream):
+    for t in (image, kernel, out):
+        if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+            raise ValueError("device variants need contiguous float32 CUDA tensors")
+    _check(getattr(load(), name)(C.c_void_p(image.data_ptr()), dim3(image),
+                                 C.c_void_p(kernel.data_ptr()), dim3(kernel),
+                                 C.c_void_p(out.data_ptr()), *extra, _stream_ptr(stream)))
+    return out
+
+
+def convolve_device(image, kernel, out, stream=None):
+    return _dev("clarityx_convolve_device", image, kernel, out, [], stream)
+
+
+def wiener_device(image, kernel, out, epsilon, stream=None):
+    return _dev("clarityx_wiener_device", image, kernel, out, [C.c_float(epsilon)], stream)
+
+
+def ml_device(image, kernel, out, iterations, stream=None):
+    return _dev("clarityx_ml_device", image, kernel, out, [int(iterations)], stream)
+
+
+def blind_ml_device(image, kernel, out, iterations, stream=None):
+    return _dev("clarityx_blind_ml_device", image, kernel, out, [int(iterations)], stream)
+
+
+def jvc_device(image, kernel, out, iterations, stream=None):
+    return _dev("clarityx_jvc_device", image, kernel, out, [int(iterations)], stream)

@@ -1,0 +1,479 @@
+// clarity_api.cpp -- the C ABI of libclarity.so (include/clarity.h and
+// include/clarity_ext.h).
+//
+// Public functions follow the reference contract (Clarity.h.in:123-383):
+// host buffers in and out, synchronous, ClarityResult_t codes with
+// CLARITY_SUCCESS == 5.  Inside, unpadded volumes are copied to the device
+// once and padded on the fly by the first FFT pass (the reference pads on
+// the host, src/ImagePadSpatialShift.cxx, and copies three padded volumes).
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/clarity.h"
+#include "../../include/clarity_ext.h"
+#include "engine.hpp"
+
+using clarity::Context;
+using clarity::Dims;
+using clarity::Status;
+
+namespace {
+
+std::mutex g_mu;                 // guards registration state
+int g_refcount = 0;              // src/Clarity.cxx:41 (made thread-safe)
+int g_device = 0;
+Context* g_ctx = nullptr;
+unsigned g_threads = 0;
+thread_local std::string g_last_error;
+
+// Staging buffers for the host-buffer API (grown on demand).
+struct Staging {
+  float* img = nullptr;
+  float* ker = nullptr;
+  float* out = nullptr;
+  size_t img_cap = 0, ker_cap = 0, out_cap = 0;
+} g_stage;
+
+ClarityResult_t fail(ClarityResult_t code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+ClarityResult_t report(const Status& s) {
+  if (s.ok()) return CLARITY_SUCCESS;
+  g_last_error = s.msg;
+  return s.code;
+}
+
+bool dims_ok(Clarity_Dim3 d) { return d.x > 0 && d.y > 0 && d.z > 0; }
+
+long long nvox(Clarity_Dim3 d) { return (long long)d.x * d.y * d.z; }
+
+Dims to_dims(Clarity_Dim3 d) { return Dims{d.x, d.y, d.z}; }
+
+Status grow(float** p, size_t* cap, size_t n) {
+  if (*cap >= n && *p) return Status::Ok();
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  cudaError_t e = clarity::dev_alloc((void**)p, sizeof(float) * n);
+  if (e != cudaSuccess) return clarity::status_from_cuda(e, "staging allocation");
+  *cap = n;
+  return Status::Ok();
+}
+
+void free_staging() {
+  cudaFree(g_stage.img);
+  cudaFree(g_stage.ker);
+  cudaFree(g_stage.out);
+  g_stage = Staging();
+}
+
+// Common path of the host-buffer algorithms: validate, upload, run, download.
+template <class Run>
+ClarityResult_t host_call(const float* in, Clarity_Dim3 id, const float* ker,
+                          Clarity_Dim3 kd, float* out, Run run) {
+  if (!in || !ker || !out) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (!dims_ok(id) || !dims_ok(kd))
+    return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  Context* ctx;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx = g_ctx;
+  }
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device());
+  ctx->set_stream(nullptr);
+  const size_t ni = (size_t)nvox(id), nk = (size_t)nvox(kd);
+  Status s = grow(&g_stage.img, &g_stage.img_cap, ni);
+  if (s.ok()) s = grow(&g_stage.ker, &g_stage.ker_cap, nk);
+  if (s.ok()) s = grow(&g_stage.out, &g_stage.out_cap, ni);
+  if (!s.ok()) return report(s);
+  cudaStream_t st = ctx->exec_stream();
+  cudaError_t e = cudaMemcpyAsync(g_stage.img, in, sizeof(float) * ni,
+                                  cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(g_stage.ker, ker, sizeof(float) * nk,
+                        cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "host to device copy"));
+  s = run(*ctx, g_stage.img, to_dims(id), g_stage.ker, to_dims(kd), g_stage.out);
+  if (!s.ok()) return report(s);
+  e = cudaMemcpyAsync(out, g_stage.out, sizeof(float) * ni, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "device to host copy"));
+  return CLARITY_SUCCESS;
+}
+
+template <class Run>
+ClarityResult_t device_call(const float* in, Clarity_Dim3 id, const float* ker,
+                            Clarity_Dim3 kd, float* out, void* stream, Run run) {
+  if (!in || !ker || !out) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (!dims_ok(id) || !dims_ok(kd))
+    return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  Context* ctx;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx = g_ctx;
+  }
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device());
+  ctx->set_stream(static_cast<cudaStream_t>(stream));
+  Status s = run(*ctx, in, to_dims(id), ker, to_dims(kd), out);
+  ctx->set_stream(nullptr);
+  return report(s);
+}
+
+}  // namespace
+
+namespace clarity {
+Context* global_context() { return g_ctx; }
+}  // namespace clarity
+
+// ================================================================== public
+
+extern "C" {
+
+Clarity_Dim3 Clarity_Dim3FromArray(int dimArray[3]) {
+  Clarity_Dim3 d;
+  d.x = dimArray[0];
+  d.y = dimArray[1];
+  d.z = dimArray[2];
+  return d;
+}
+
+ClarityResult_t Clarity_Register(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_refcount == 0) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= g_device)
+      return fail(CLARITY_INVALID_OPERATION, "no CUDA device available");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, g_device);
+    if (e != cudaSuccess) return fail(CLARITY_INVALID_OPERATION, cudaGetErrorString(e));
+    if (prop.major != 10)
+      return fail(CLARITY_INVALID_OPERATION,
+                  std::string("device is not sm_100 class: ") + prop.name);
+    g_ctx = new Context(g_device);
+    if (std::getenv("CLARITY_LOG"))
+      std::fprintf(stderr, "clarity: device %d '%s', %zu MB\n", g_device, prop.name,
+                   (size_t)(prop.totalGlobalMem >> 20));
+  }
+  g_refcount++;
+  return CLARITY_SUCCESS;
+}
+
+ClarityResult_t Clarity_UnRegister(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_refcount <= 0) return fail(CLARITY_INVALID_OPERATION, "not registered");
+  if (--g_refcount == 0) {
+    {
+      std::lock_guard<std::mutex> lk2(g_ctx->mu);
+      cudaSetDevice(g_ctx->device());
+      cudaDeviceSynchronize();
+      free_staging();
+    }
+    delete g_ctx;
+    g_ctx = nullptr;
+  }
+  return CLARITY_SUCCESS;
+}
+
+ClarityResult_t Clarity_SetNumberOfThreads(unsigned n) {
+  g_threads = n;
+  return CLARITY_SUCCESS;
+}
+
+ClarityResult_t Clarity_ImagePadSpatialShift(float* dst, Clarity_Dim3 dstDim,
+                                             float* src, Clarity_Dim3 srcDim,
+                                             int shift[3], float fillValue) {
+  if (!dst || !src || !shift) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (!dims_ok(dstDim) || !dims_ok(srcDim))
+    return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  // src/ImagePadSpatialShift.cxx:42-66
+  for (int dk = 0; dk < dstDim.z; dk++) {
+    int sk = dk - shift[2];
+    if (sk < 0) sk += dstDim.z;
+    sk = sk % dstDim.z;
+    const bool wk = sk >= 0 && sk < srcDim.z;
+    for (int dj = 0; dj < dstDim.y; dj++) {
+      int sj = dj - shift[1];
+      if (sj < 0) sj += dstDim.y;
+      sj = sj % dstDim.y;
+      const bool wj = sj >= 0 && sj < srcDim.y;
+      float* drow = dst + ((long long)dk * dstDim.y + dj) * dstDim.x;
+      const float* srow = src + ((long long)sk * srcDim.y + sj) * srcDim.x;
+      for (int di = 0; di < dstDim.x; di++) {
+        int si = di - shift[0];
+        if (si < 0) si += dstDim.x;
+        si = si % dstDim.x;
+        const bool wi = si >= 0 && si < srcDim.x;
+        drow[di] = (wi && wj && wk) ? srow[si] : fillValue;
+      }
+    }
+  }
+  return CLARITY_SUCCESS;
+}
+
+ClarityResult_t Clarity_ImageClip(float* dst, Clarity_Dim3 dstDim, float* src,
+                                  Clarity_Dim3 srcDim) {
+  if (!dst || !src) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (!dims_ok(dstDim) || !dims_ok(srcDim))
+    return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  if (dstDim.x > srcDim.x || dstDim.y > srcDim.y || dstDim.z > srcDim.z)
+    return fail(CLARITY_INVALID_ARGUMENT, "clip box larger than source");
+  for (int k = 0; k < dstDim.z; k++)
+    for (int j = 0; j < dstDim.y; j++)
+      std::memcpy(dst + ((long long)k * dstDim.y + j) * dstDim.x,
+                  src + ((long long)k * srcDim.y + j) * srcDim.x,
+                  sizeof(float) * dstDim.x);
+  return CLARITY_SUCCESS;
+}
+
+char* Clarity_ResultString(ClarityResult_t result) {
+  // src/Clarity.cxx:116-150
+  switch (result) {
+    case CLARITY_FFT_FAILED: return const_cast<char*>("CLARITY_FFT_FAILED");
+    case CLARITY_OUT_OF_MEMORY: return const_cast<char*>("CLARITY_OUT_OF_MEMORY");
+    case CLARITY_DEVICE_OUT_OF_MEMORY:
+      return const_cast<char*>("CLARITY_DEVICE_OUT_OF_MEMORY");
+    case CLARITY_INVALID_OPERATION: return const_cast<char*>("CLARITY_INVALID_OPERATION");
+    case CLARITY_INVALID_ARGUMENT: return const_cast<char*>("CLARITY_INVALID_ARGUMENT");
+    case CLARITY_SUCCESS: return const_cast<char*>("CLARITY_SUCCESS");
+    default: return const_cast<char*>("<unknown Clarity result>");
+  }
+}
+
+ClarityResult_t Clarity_WienerDeconvolve(float* inImage, Clarity_Dim3 imageDim,
+                                         float* kernelImage, Clarity_Dim3 kernelDim,
+                                         float* outImage, float epsilon) {
+  return host_call(inImage, imageDim, kernelImage, kernelDim, outImage,
+                   [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                       float* o) { return clarity::run_wiener(c, i, id, k, kd, o, epsilon); });
+}
+
+ClarityResult_t Clarity_JansenVanCittertDeconvolve(float* inImage, Clarity_Dim3 imageDim,
+                                                   float* kernelImage,
+                                                   Clarity_Dim3 kernelDim,
+                                                   float* outImage, int iterations) {
+  return host_call(inImage, imageDim, kernelImage, kernelDim, outImage,
+                   [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                       float* o) {
+                     return clarity::run_jvc(c, i, id, k, kd, o, iterations, 0.f,
+                                             nullptr, 0);
+                   });
+}
+
+ClarityResult_t Clarity_SmoothedJansenVanCittertDeconvolve(
+    float* inImage, Clarity_Dim3 imageDim, float* kernelImage, Clarity_Dim3 kernelDim,
+    float* outImage, unsigned iterations, unsigned smoothInterval,
+    float* smoothSigma[3]) {
+  float sig[3] = {0.f, 0.f, 0.f};
+  bool smooth = smoothSigma != nullptr && smoothInterval > 0;
+  if (smooth) {
+    for (int d = 0; d < 3; ++d) {
+      if (!smoothSigma[d]) { smooth = false; break; }
+      sig[d] = *smoothSigma[d];
+    }
+  }
+  return host_call(inImage, imageDim, kernelImage, kernelDim, outImage,
+                   [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                       float* o) {
+                     return clarity::run_jvc(c, i, id, k, kd, o, (int)iterations, 0.f,
+                                             smooth ? sig : nullptr,
+                                             smooth ? (int)smoothInterval : 0);
+                   });
+}
+
+ClarityResult_t Clarity_IDivergenceDeconvolve(float* inImage, Clarity_Dim3 imageDim,
+                                              float* kernelImage, Clarity_Dim3 kernelDim,
+                                              float* outImage) {
+  // The reference body writes zeros (src/IDivergenceDeconvolve.cxx:59-72).
+  if (!inImage || !kernelImage || !outImage)
+    return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (!dims_ok(imageDim) || !dims_ok(kernelDim))
+    return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  std::memset(outImage, 0, sizeof(float) * (size_t)nvox(imageDim));
+  return CLARITY_SUCCESS;
+}
+
+ClarityResult_t Clarity_MaximumLikelihoodDeconvolve(float* inImage, Clarity_Dim3 imageDim,
+                                                    float* kernelImage,
+                                                    Clarity_Dim3 kernelDim,
+                                                    float* outImage, int iterations) {
+  return host_call(inImage, imageDim, kernelImage, kernelDim, outImage,
+                   [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                       float* o) { return clarity::run_rl(c, i, id, k, kd, o, iterations); });
+}
+
+ClarityResult_t Clarity_BlindMaximumLikelihoodDeconvolve(float* inImage,
+                                                         Clarity_Dim3 imageDim,
+                                                         float* kernelImage,
+                                                         Clarity_Dim3 kernelDim,
+                                                         float* outImage, int iterations) {
+  return host_call(inImage, imageDim, kernelImage, kernelDim, outImage,
+                   [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                       float* o) {
+                     return clarity::run_blind(c, i, id, k, kd, o, iterations);
+                   });
+}
+
+ClarityResult_t Clarity_Convolve(float* inImage, Clarity_Dim3 imageDim, float* kernel,
+                                 Clarity_Dim3 kernelDim, float* outImage) {
+  return host_call(inImage, imageDim, kernel, kernelDim, outImage,
+                   [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                       float* o) { return clarity::run_convolve(c, i, id, k, kd, o); });
+}
+
+// ============================================================== extensions
+
+const char* clarityx_last_error(void) { return g_last_error.c_str(); }
+
+ClarityResult_t clarityx_set_device(int device) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_refcount > 0) return fail(CLARITY_INVALID_OPERATION, "already registered");
+  if (device < 0) return fail(CLARITY_INVALID_ARGUMENT, "negative device");
+  g_device = device;
+  return CLARITY_SUCCESS;
+}
+
+void clarityx_inject_device_alloc_failure(int countdown) {
+  clarity::set_alloc_failure_countdown(countdown);
+}
+
+ClarityResult_t clarityx_trim(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_ctx) return fail(CLARITY_INVALID_OPERATION, "not registered");
+  std::lock_guard<std::mutex> lk2(g_ctx->mu);
+  cudaSetDevice(g_ctx->device());
+  cudaDeviceSynchronize();
+  g_ctx->release_workspaces();
+  free_staging();
+  return CLARITY_SUCCESS;
+}
+
+ClarityResult_t clarityx_synchronize(void* stream) {
+  Context* ctx = g_ctx;
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "not registered");
+  cudaSetDevice(ctx->device());
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream();
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "synchronize"));
+  return CLARITY_SUCCESS;
+}
+
+ClarityResult_t clarityx_convolve_device(const float* image, Clarity_Dim3 imageDim,
+                                         const float* kernel, Clarity_Dim3 kernelDim,
+                                         float* out, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) { return clarity::run_convolve(c, i, id, k, kd, o); });
+}
+
+ClarityResult_t clarityx_wiener_device(const float* image, Clarity_Dim3 imageDim,
+                                       const float* kernel, Clarity_Dim3 kernelDim,
+                                       float* out, float epsilon, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_wiener(c, i, id, k, kd, o, epsilon);
+                     });
+}
+
+ClarityResult_t clarityx_ml_device(const float* image, Clarity_Dim3 imageDim,
+                                   const float* kernel, Clarity_Dim3 kernelDim,
+                                   float* out, int iterations, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_rl(c, i, id, k, kd, o, iterations);
+                     });
+}
+
+ClarityResult_t clarityx_blind_ml_device(const float* image, Clarity_Dim3 imageDim,
+                                         const float* kernel, Clarity_Dim3 kernelDim,
+                                         float* out, int iterations, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_blind(c, i, id, k, kd, o, iterations);
+                     });
+}
+
+ClarityResult_t clarityx_jvc_device(const float* image, Clarity_Dim3 imageDim,
+                                    const float* kernel, Clarity_Dim3 kernelDim,
+                                    float* out, int iterations, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_jvc(c, i, id, k, kd, o, iterations, 0.f,
+                                               nullptr, 0);
+                     });
+}
+
+ClarityResult_t clarityx_idivergence(const float* g, const float* ghat, long long n,
+                                     double* result) {
+  if (!g || !ghat || !result) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (n <= 0) return fail(CLARITY_INVALID_ARGUMENT, "n <= 0");
+  Context* ctx = g_ctx;
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device());
+  ctx->set_stream(nullptr);
+  float *dg = nullptr, *dh = nullptr;
+  cudaError_t e = clarity::dev_alloc((void**)&dg, sizeof(float) * n);
+  if (e == cudaSuccess) e = clarity::dev_alloc((void**)&dh, sizeof(float) * n);
+  cudaStream_t st = ctx->exec_stream();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dg, g, sizeof(float) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dh, ghat, sizeof(float) * n, cudaMemcpyHostToDevice, st);
+  Status s = (e == cudaSuccess) ? clarity::run_idivergence(*ctx, dg, dh, n, result)
+                                : clarity::status_from_cuda(e, "idivergence staging");
+  cudaFree(dg);
+  cudaFree(dh);
+  return report(s);
+}
+
+ClarityResult_t clarityx_plan_info(Clarity_Dim3 w, int* f, int nf) {
+  if (!f || nf <= 0) return fail(CLARITY_INVALID_ARGUMENT, "NULL fields");
+  if (!dims_ok(w)) return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  clarity::VolPlan P;
+  std::string why;
+  if (!clarity::make_plan(w.x, w.y, w.z, &P, &why))
+    return fail(CLARITY_INVALID_ARGUMENT, why);
+  const int v[16] = {P.M, P.XS, P.Ay, P.By, P.G, P.W, P.KG, P.xy_blocks, P.z_blocks,
+                     P.xy_smem, P.z_smem, P.ax.npass, P.ayB.npass, P.az.npass,
+                     P.xmode, (int)(P.spec_elems / 1024)};
+  for (int i = 0; i < nf && i < 16; ++i) f[i] = v[i];
+  return CLARITY_SUCCESS;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------- benchmark probes
+extern "C" {
+
+CLARITY_API long long clarityx_launch_count(void) { return clarity::launch_count(); }
+
+CLARITY_API void clarityx_timing_enable(int on) { clarity::timing_enable(on != 0); }
+
+CLARITY_API void clarityx_timing_collect(double* ms, long long* counts, int n) {
+  double m[clarity::KK_COUNT];
+  long long c[clarity::KK_COUNT];
+  clarity::timing_collect(m, c);
+  for (int i = 0; i < n && i < clarity::KK_COUNT; ++i) {
+    if (ms) ms[i] = m[i];
+    if (counts) counts[i] = c[i];
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,778 @@
+// engine.cu -- planner, device context and the deconvolution algorithms of
+// the Clarity path on sm_100a.
+//
+// Reference: the per-algorithm drivers src/MaximumLikelihoodDeconvolve.cxx
+// :160-250, src/WienerDeconvolve.cxx:130-206,
+// src/JansenVanCittertDeconvolve.cxx:199-307, src/Convolve.cxx:41-115 and
+// src/BlindMaximumLikelihoodDeconvolve.cxx:102-148, which allocate, plan and
+// free on every call and synchronise after every kernel.  Here plans and
+// buffers are cached per work box, every step is a fused FFT pass, and an
+// RL iteration is five kernel launches with no host round trip.
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "engine.hpp"
+#include "launch.cuh"
+#include "ops.cuh"
+#include "passes.cuh"
+
+namespace clarity {
+
+// ------------------------------------------------------------------ errors
+Status status_from_cuda(cudaError_t e, const char* what) {
+  Status s;
+  if (e == cudaSuccess) return s;
+  s.code = (e == cudaErrorMemoryAllocation) ? CLARITY_DEVICE_OUT_OF_MEMORY
+                                            : CLARITY_INVALID_OPERATION;
+  s.msg = std::string(what) + ": " + cudaGetErrorString(e);
+  return s;
+}
+
+
+static std::atomic<int> g_alloc_fail_countdown{0};
+
+void set_alloc_failure_countdown(int n) { g_alloc_fail_countdown.store(n); }
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+  int c = g_alloc_fail_countdown.load();
+  if (c > 0) {
+    if (g_alloc_fail_countdown.fetch_sub(1) == 1) {
+      *p = nullptr;
+      return cudaErrorMemoryAllocation;  // injected on the host
+    }
+  }
+  return cudaMalloc(p, bytes ? bytes : 16);
+}
+
+// ------------------------------------------------------- launch accounting
+static std::atomic<long long> g_launches{0};
+static std::atomic<bool> g_timing{false};
+static std::mutex g_timing_mu;
+struct EventPair {
+  int kind;
+  cudaEvent_t a, b;
+};
+static std::vector<EventPair> g_events;   // recorded pairs
+static std::vector<cudaEvent_t> g_event_pool;
+static cudaEvent_t g_pending[KK_COUNT];
+
+static cudaEvent_t take_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void note_launch_begin(int kind, cudaStream_t st) {
+  g_launches.fetch_add(1);
+  if (!g_timing.load()) return;
+  std::lock_guard<std::mutex> lk(g_timing_mu);
+  cudaEvent_t e = take_event();
+  cudaEventRecord(e, st);
+  g_pending[kind] = e;
+}
+
+void note_launch_end(int kind, cudaStream_t st) {
+  if (!g_timing.load()) return;
+  std::lock_guard<std::mutex> lk(g_timing_mu);
+  cudaEvent_t e = take_event();
+  cudaEventRecord(e, st);
+  g_events.push_back(EventPair{kind, g_pending[kind], e});
+}
+
+long long launch_count() { return g_launches.load(); }
+
+static inline void count_small() { g_launches.fetch_add(1); }
+
+void timing_enable(bool on) { g_timing.store(on); }
+
+void timing_collect(double* ms, long long* counts) {
+  std::lock_guard<std::mutex> lk(g_timing_mu);
+  for (int k = 0; k < KK_COUNT; ++k) { ms[k] = 0; counts[k] = 0; }
+  for (auto& p : g_events) {
+    cudaEventSynchronize(p.b);
+    float t = 0;
+    cudaEventElapsedTime(&t, p.a, p.b);
+    ms[p.kind] += t;
+    counts[p.kind] += 1;
+    g_event_pool.push_back(p.a);
+    g_event_pool.push_back(p.b);
+  }
+  g_events.clear();
+}
+
+// ----------------------------------------------------------------- planner
+static void search_axis(int n, int depth, int* cur, int* best, int* best_len,
+                        int* best_max) {
+  if (n == 1) {
+    int mx = 0;
+    for (int i = 0; i < depth; ++i) mx = std::max(mx, cur[i]);
+    if (depth < *best_len || (depth == *best_len && mx < *best_max)) {
+      *best_len = depth;
+      *best_max = mx;
+      for (int i = 0; i < depth; ++i) best[i] = cur[i];
+    }
+    return;
+  }
+  if (depth >= kMaxPasses || depth + 1 > *best_len) return;
+  for (int r : kRadixSet) {
+    if (n % r == 0) {
+      // keep radices non-increasing to avoid permutations of one factor set
+      if (depth > 0 && r > cur[depth - 1]) continue;
+      cur[depth] = r;
+      search_axis(n / r, depth + 1, cur, best, best_len, best_max);
+    }
+  }
+}
+
+static bool plan_axis(int n, AxisPlan* A) {
+  std::memset(A, 0, sizeof(*A));
+  A->n = n;
+  if (n == 1) return true;
+  int cur[kMaxPasses], best[kMaxPasses];
+  int best_len = kMaxPasses + 1, best_max = INT_MAX;
+  search_axis(n, 0, cur, best, &best_len, &best_max);
+  if (best_len > kMaxPasses) return false;
+  A->npass = best_len;
+  int len = n;
+  for (int s = 0; s < best_len; ++s) {
+    A->radix[s] = best[s];
+    A->len[s] = len;
+    A->span[s] = len / best[s];
+    len /= best[s];
+  }
+  return true;
+}
+
+static int ctz(int v) {
+  int c = 0;
+  while (v && !(v & 1)) { v >>= 1; ++c; }
+  return c;
+}
+
+static constexpr int kSmemMax = 200 * 1024;
+static constexpr int kSmemPerSM = 228 * 1024;
+
+bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
+  VolPlan P;
+  std::memset(&P, 0, sizeof(P));
+  P.nx = nx; P.ny = ny; P.nz = nz;
+  P.xmode = (nx % 2 == 0) ? 0 : 1;
+  P.M = P.xmode == 0 ? nx / 2 : nx;
+  P.XS = P.xmode == 0 ? P.M + 1 : nx;
+  if (P.xmode == 0)
+    P.items = (P.M % 2 == 0) ? std::max(P.M / 2, 1) : (P.M + 1) / 2;
+  else
+    P.items = nx;
+  if (!plan_axis(P.M, &P.ax)) {
+    if (why) *why = "x length " + std::to_string(nx) + " has an unsupported factor";
+    return false;
+  }
+  if (!plan_axis(nz, &P.az)) {
+    if (why) *why = "z length " + std::to_string(nz) + " has an unsupported factor";
+    return false;
+  }
+  // x row padding in the XY shared memory
+  if (P.ax.npass <= 1 || (P.ax.span[0] & 1)) P.padShift = 30;
+  else P.padShift = ctz(P.ax.span[0]);
+  {
+    const int last = P.M - 1;
+    int rs = last + (last >> P.padShift) + 1;
+    if (rs % 2 == 0) rs += 1;
+    P.rowStride = rs;
+  }
+  double best_score = -1e300;
+  VolPlan best = P;
+  bool found = false;
+  std::vector<int> ays = {1};
+  for (int r : kRadixSet) ays.push_back(r);
+  for (int ay : ays) {
+    if (ny % ay) continue;
+    const int by = ny / ay;
+    AxisPlan ab;
+    if (!plan_axis(by, &ab)) continue;
+    for (int W : {1, 2, 4, 8}) {
+      const long long zsm = (long long)nz * by * W * 8;
+      if (zsm > kSmemMax) continue;
+      for (int G = 1; G <= 16; ++G) {
+        if (by % G) continue;
+        const long long xysm = (long long)G * ay * P.rowStride * 8;
+        if (xysm > kSmemMax) continue;
+        const int KG = (P.XS + W - 1) / W;
+        const long long xy_blocks = (long long)nz * (by / G);
+        const long long z_blocks = (long long)ay * KG;
+        const int occ_xy = std::min(8, (int)(kSmemPerSM / (xysm + 1024)));
+        const int occ_z = std::min(8, (int)(kSmemPerSM / (zsm + 1024)));
+        const double seg = (double)G * W * 8;
+        double score = 0;
+        score += 10.0 * std::min(std::min(occ_xy, occ_z), 3);
+        score += seg >= 32 ? 6.0 : seg / 32.0 * 6.0;
+        score += (xy_blocks >= 296 ? 3.0 : 3.0 * xy_blocks / 296.0);
+        score += (z_blocks >= 296 ? 3.0 : 3.0 * z_blocks / 296.0);
+        score -= 4.0 * ((double)KG * W / P.XS - 1.0);
+        score -= 0.05 * std::abs(ay - 16);
+        score -= 0.02 * G;  // prefer fewer rows per tile at equal merit
+        if (score > best_score) {
+          best_score = score;
+          best = P;
+          best.Ay = ay; best.By = by; best.G = G; best.W = W; best.KG = KG;
+          best.ayB = ab;
+          best.xy_smem = (int)xysm;
+          best.z_smem = (int)zsm;
+          best.xy_blocks = (int)xy_blocks;
+          best.z_blocks = (int)z_blocks;
+          found = true;
+        }
+      }
+    }
+  }
+  if (!found) {
+    if (why) *why = "no tiling of y=" + std::to_string(ny) + ", z=" + std::to_string(nz) +
+                    " fits in shared memory with the supported radices";
+    return false;
+  }
+  P = best;
+  P.xy_threads = 256;
+  P.z_threads = 256;
+  P.spec_elems = (long long)P.Ay * P.KG * P.nz * P.By * P.W;
+  // twiddle buffer layout
+  int off = 0;
+  P.ax.tw_off = off; off += std::max(P.M, 1);
+  P.ayB.tw_off = off; off += std::max(P.By, 1);
+  P.az.tw_off = off; off += std::max(P.nz, 1);
+  P.tw_r2c_off = off; off += P.M / 2 + 1;
+  P.tw_ny_off = off; off += P.ny;
+  P.twiddle_count = off;
+  P.xrev_off = 0;
+  P.xrev_count = P.M;
+  *out = P;
+  return true;
+}
+
+// ------------------------------------------------------------ small kernels
+struct TwTable {
+  int off, n, count;
+};
+
+// w_n^t = exp(-2 pi i t / n), evaluated in FP64 with sincospi and rounded.
+__global__ void k_gen_twiddles(float2* tw, const TwTable* tabs, int ntab) {
+  for (int k = 0; k < ntab; ++k) {
+    const TwTable T = tabs[k];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T.count;
+         t += gridDim.x * blockDim.x) {
+      double s, c;
+      sincospi(2.0 * (double)t / (double)T.n, &s, &c);
+      tw[T.off + t] = make_float2((float)c, (float)(-s));
+    }
+  }
+}
+
+// FP64 partial sums of a float array (grid-stride; fixed grid -> fixed order).
+__global__ void k_reduce_sum(const float* __restrict__ a, long long n,
+                             double* __restrict__ partial) {
+  double acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    acc += (double)a[i];
+  block_sum_store(acc, partial);
+}
+
+__device__ __forceinline__ double block_total(const double* partial, int np) {
+  double acc = 0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partial[i];
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  double t = 0;
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) t += red[w];
+  }
+  return t;  // valid in thread 0
+}
+
+// sum -> dout[0]
+__global__ void k_finish_sum(const double* partial, int np, double* dout) {
+  const double t = block_total(partial, np);
+  if (threadIdx.x == 0) dout[0] = t;
+}
+
+// RL flux scale (src/MaximumLikelihoodDeconvolve.cxx:73-78):
+// scale = energy / newEnergy with both rounded to float first, as the
+// reference holds them in floats.
+__global__ void k_finish_rl_scale(const double* partial, int np,
+                                  const double* energy, double* sum_out,
+                                  float* scale_out) {
+  const double t = block_total(partial, np);
+  if (threadIdx.x == 0) {
+    sum_out[0] = t;
+    scale_out[0] = (float)energy[0] / (float)t;
+  }
+}
+
+// 1 / sum, in float (Clarity_NormalizeArray, src/ComputePrimitives.cxx:197-209)
+__global__ void k_finish_inverse(const double* partial, int np, float* out) {
+  const double t = block_total(partial, np);
+  if (threadIdx.x == 0) out[0] = 1.0f / (float)t;
+}
+
+// Crop the work box to the image region, times an optional device scale.
+__global__ void k_clip(const float* __restrict__ w, int nx, int ny,
+                       float* __restrict__ out, int X, int Y, int Z,
+                       const float* __restrict__ scale) {
+  const long long n = (long long)X * Y * Z;
+  const float s = scale ? *scale : 1.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % X);
+    const long long r = i / X;
+    const int y = (int)(r % Y);
+    const int z = (int)(r / Y);
+    const float v = w[((long long)z * ny + y) * nx + x];
+    out[i] = scale ? s * v : v;
+  }
+}
+
+__global__ void k_copy(const float* __restrict__ a, float* __restrict__ b,
+                       long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+// max of a float array: block maxima then a single-block finish.
+__global__ void k_reduce_max(const float* __restrict__ a, long long n,
+                             float* __restrict__ partial) {
+  float m = -INFINITY;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, a[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ float red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) t = fmaxf(t, red[w]);
+    partial[blockIdx.x] = t;
+  }
+}
+
+// JVC constants from the image maximum (src/JansenVanCittertDeconvolve.cxx
+// :128-129): A = 0.5 max, invASq = 1 / (A A).  out[0] = A, out[1] = invASq.
+__global__ void k_finish_jvc(const float* partial, int np, float* out) {
+  if (threadIdx.x == 0) {
+    float m = partial[0];
+    for (int i = 1; i < np; ++i) m = fmaxf(m, partial[i]);
+    const float A = 0.5f * m;
+    out[0] = A;
+    out[1] = 1.0f / (A * A);
+  }
+}
+
+// I-divergence partials: g ln(g/ghat) + ghat - g (0 ln 0 = 0), FP64.
+__global__ void k_idiv(const float* __restrict__ g, const float* __restrict__ gh,
+                       long long n, double* __restrict__ partial) {
+  double acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double a = g[i], b = gh[i];
+    if (a > 0) {
+      if (b > 0) acc += a * log(a / b) + b - a;
+    } else {
+      acc += b - a;
+    }
+  }
+  block_sum_store(acc, partial);
+}
+
+static constexpr int kReduceBlocks = 592;  // 4 x 148 SMs
+
+// --------------------------------------------------------------- context
+Context::Context(int device) : device_(device) {
+  cudaSetDevice(device);
+  cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+}
+
+Context::~Context() {
+  cudaSetDevice(device_);
+  release_workspaces();
+  for (auto& kv : plans_) {
+    cudaFree(kv.second->tw);
+    cudaFree(kv.second->xrev);
+  }
+  plans_.clear();
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Context::release_workspaces() {
+  Workspace& w = ws_;
+  cudaFree(w.S); cudaFree(w.H); cudaFree(w.u); cudaFree(w.img); cudaFree(w.ker);
+  cudaFree(w.partial); cudaFree(w.dscal); cudaFree(w.fscal);
+  w = Workspace();
+}
+
+Status Context::plan(const Dims& wd, const PlanEntry** out) {
+  auto key = std::make_tuple(wd.x, wd.y, wd.z);
+  auto it = plans_.find(key);
+  if (it != plans_.end()) {
+    *out = it->second.get();
+    return Status::Ok();
+  }
+  auto pe = std::make_unique<PlanEntry>();
+  std::string why;
+  if (!make_plan(wd.x, wd.y, wd.z, &pe->P, &why)) {
+    Status s;
+    s.code = CLARITY_INVALID_ARGUMENT;
+    s.msg = "unsupported work box " + std::to_string(wd.x) + "x" +
+            std::to_string(wd.y) + "x" + std::to_string(wd.z) + ": " + why;
+    return s;
+  }
+  const VolPlan& P = pe->P;
+  CL_CHECK(dev_alloc((void**)&pe->tw, sizeof(float2) * P.twiddle_count));
+  CL_CHECK(dev_alloc((void**)&pe->xrev, sizeof(int) * std::max(P.xrev_count, 1)));
+  // digit-reversed slot of each natural x frequency after the DIF passes
+  std::vector<int> rev(std::max(P.M, 1));
+  for (int k = 0; k < P.M; ++k) {
+    int rem = k, pos = 0;
+    for (int s = 0; s < P.ax.npass; ++s) {
+      const int d = rem % P.ax.radix[s];
+      rem /= P.ax.radix[s];
+      pos += d * P.ax.span[s];
+    }
+    rev[k] = pos;
+  }
+  if (P.M == 1) rev[0] = 0;
+  std::vector<TwTable> tabs = {
+      {P.ax.tw_off, std::max(P.M, 1), std::max(P.M, 1)},
+      {P.ayB.tw_off, std::max(P.By, 1), std::max(P.By, 1)},
+      {P.az.tw_off, std::max(P.nz, 1), std::max(P.nz, 1)},
+      {P.tw_r2c_off, P.nx, P.M / 2 + 1},
+      {P.tw_ny_off, P.ny, P.ny},
+  };
+  TwTable* dtabs = nullptr;
+  CL_CHECK(dev_alloc((void**)&dtabs, sizeof(TwTable) * tabs.size()));
+  cudaStream_t st = exec_stream();
+  CL_CHECK(cudaMemcpyAsync(pe->xrev, rev.data(), sizeof(int) * rev.size(),
+                           cudaMemcpyHostToDevice, st));
+  CL_CHECK(cudaMemcpyAsync(dtabs, tabs.data(), sizeof(TwTable) * tabs.size(),
+                           cudaMemcpyHostToDevice, st));
+  k_gen_twiddles<<<64, 256, 0, st>>>(pe->tw, dtabs, (int)tabs.size());
+  CL_CHECK(cudaGetLastError());
+  CL_CHECK(cudaStreamSynchronize(st));
+  cudaFree(dtabs);
+  *out = pe.get();
+  plans_[key] = std::move(pe);
+  return Status::Ok();
+}
+
+template <class T>
+static Status ensure(T** p, long long* cap, long long need) {
+  if (*cap >= need && *p) return Status::Ok();
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  CL_CHECK(dev_alloc((void**)p, sizeof(T) * (size_t)need));
+  *cap = need;
+  return Status::Ok();
+}
+
+Status Context::workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
+                          Workspace** out) {
+  Workspace& w = ws_;
+  const VolPlan& P = pe.P;
+  long long sc = w.spec_cap;
+  Status s;
+  if (w.spec_cap < P.spec_elems || !w.S || !w.H) {
+    cudaFree(w.S); cudaFree(w.H);
+    w.S = w.H = nullptr;
+    w.spec_cap = 0;
+    CL_CHECK(dev_alloc((void**)&w.S, sizeof(float2) * (size_t)P.spec_elems));
+    CL_CHECK(dev_alloc((void**)&w.H, sizeof(float2) * (size_t)P.spec_elems));
+    w.spec_cap = P.spec_elems;
+  }
+  (void)sc;
+  s = ensure(&w.u, &w.work_cap, P.n_real());
+  if (!s.ok()) return s;
+  long long ic = (long long)w.img_cap, kc = (long long)w.ker_cap;
+  s = ensure(&w.img, &ic, img.n());
+  if (!s.ok()) return s;
+  w.img_cap = (size_t)ic;
+  s = ensure(&w.ker, &kc, ker.n());
+  if (!s.ok()) return s;
+  w.ker_cap = (size_t)kc;
+  long long pc = w.partial_cap;
+  s = ensure(&w.partial, &pc, std::max<long long>(std::max(P.xy_blocks, kReduceBlocks), 1));
+  if (!s.ok()) return s;
+  w.partial_cap = (int)pc;
+  if (!w.dscal) CL_CHECK(dev_alloc((void**)&w.dscal, sizeof(double) * 16));
+  if (!w.fscal) CL_CHECK(dev_alloc((void**)&w.fscal, sizeof(float) * 16));
+  *out = &w;
+  return Status::Ok();
+}
+
+// Launch wrappers are instantiated in the kern_*.cu translation units.
+CLARITY_EXTERN_LAUNCHES
+
+#define CL_TRY(expr)              \
+  do {                            \
+    Status s_ = (expr);           \
+    if (!s_.ok()) return s_;      \
+  } while (0)
+
+static PaddedSrc padded(const float* src, Dims sd, Dims wd, int sx, int sy,
+                        int sz) {
+  PaddedSrc p;
+  p.src = src;
+  p.X = sd.x; p.Y = sd.y; p.Z = sd.z;
+  p.sx = sx; p.sy = sy; p.sz = sz;
+  p.nx = wd.x; p.ny = wd.y; p.nz = wd.z;
+  return p;
+}
+
+static Dims work_dims(Dims id, Dims kd) {
+  return Dims{id.x + kd.x, id.y + kd.y, id.z + kd.z};
+}
+
+static float inv_volume(const Dims& wd) {
+  // src/Convolve.cxx:199: 1.0f / ((float) nz*ny*nx)
+  return 1.0f / ((float)wd.z * wd.y * wd.x);
+}
+
+// OTF: R2C of the kernel padded to the work box and shifted by -kernelDim/2
+// (src/MaximumLikelihoodDeconvolve.cxx:286-289,181), in the S layout.
+static Status make_otf(Context& ctx, const PlanEntry& pe, const float* ker,
+                       Dims kd, Dims wd, float2* H, const float* scale) {
+  ProPadded pro;
+  pro.p = padded(ker, kd, wd, -kd.x / 2, -kd.y / 2, -kd.z / 2);
+  pro.scale = scale;
+  pro.xmode = pe.P.xmode;
+  CL_TRY(xy_forward(ctx, pe, pro, H));
+  CL_TRY(z_pass(ctx, pe, ModForward{}, H, H));
+  return Status::Ok();
+}
+
+static Status setup(Context& ctx, Dims id, Dims kd, const PlanEntry** pe,
+                    Workspace** ws, Dims* wd) {
+  *wd = work_dims(id, kd);
+  CL_TRY(ctx.plan(*wd, pe));
+  CL_TRY(ctx.workspace(**pe, id, kd, ws));
+  return Status::Ok();
+}
+
+static Status reduce_sum_into(Context& ctx, const float* a, long long n,
+                              double* partial, double* dout) {
+  cudaStream_t st = ctx.exec_stream();
+  count_small();
+  k_reduce_sum<<<kReduceBlocks, 256, 0, st>>>(a, n, partial);
+  count_small();
+  k_finish_sum<<<1, 256, 0, st>>>(partial, kReduceBlocks, dout);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+Status run_convolve(Context& ctx, const float* img, Dims id, const float* ker,
+                    Dims kd, float* out) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  const VolPlan& P = pe->P;
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  ProPadded pro{padded(img, id, wd, 0, 0, 0), nullptr, P.xmode};
+  CL_TRY(xy_forward(ctx, *pe, pro, ws->S));
+  CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, inv_volume(wd)}, ws->S, ws->S));
+  EpiClip epi{out, id.x, id.y, id.z, nullptr, P.xmode};
+  CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
+  return Status::Ok();
+}
+
+Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
+                  Dims kd, float* out, float eps) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  const VolPlan& P = pe->P;
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  ProPadded pro{padded(img, id, wd, 0, 0, 0), nullptr, P.xmode};
+  CL_TRY(xy_forward(ctx, *pe, pro, ws->S));
+  CL_TRY(z_pass(ctx, *pe, ModWiener{ws->H, eps, inv_volume(wd)}, ws->S, ws->S));
+  EpiClip epi{out, id.x, id.y, id.z, nullptr, P.xmode};
+  CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
+  return Status::Ok();
+}
+
+// Richardson-Lucy, five fused passes per iteration:
+//   P1 xy-forward of cur = s*u (or the padded image)      -> S
+//   P2 z pass: y0/z forward, * OTF / N, inverse           -> S   (h * cur)
+//   P3 xy inverse, r = g / (h*cur) with the 1e-5 guard, xy forward -> S
+//   P4 z pass again                                       -> S   (h * r)
+//   P5 xy inverse, u' = cur * (h*r), FP64 partial sums    -> u
+// then s = E / sum(u') on the device (deferred flux rescale).
+static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
+                      const float* img, Dims id, Dims wd, int iters,
+                      bool rescale) {
+  const VolPlan& P = pe.P;
+  cudaStream_t st = ctx.exec_stream();
+  const PaddedSrc g = padded(img, id, wd, 0, 0, 0);
+  const WorkVol wv{wd.x, wd.y, wd.z};
+  const float scale_n = inv_volume(wd);
+  float* sdev = ws.fscal;  // deferred flux scale
+  if (rescale) CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
+  for (int k = 0; k < iters; ++k) {
+    const bool first = (k == 0);
+    const float* cur_scale = (first || !rescale) ? nullptr : sdev;
+    if (first) {
+      CL_TRY(xy_forward(ctx, pe, ProPadded{g, nullptr, P.xmode}, ws.S));
+    } else {
+      CL_TRY(xy_forward(ctx, pe, ProWork{ws.u, cur_scale, wv, P.xmode}, ws.S));
+    }
+    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n}, ws.S, ws.S));
+    CL_TRY(xy_inv_fwd(ctx, pe, MidRLRatio{g, P.xmode}, ws.S));
+    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n}, ws.S, ws.S));
+    EpiRLProduct epi;
+    epi.cur = first ? nullptr : ws.u;
+    epi.g = g;
+    epi.scale = cur_scale;
+    epi.unew = ws.u;
+    epi.partial = ws.partial;
+    epi.w = wv;
+    epi.xmode = P.xmode;
+    epi.acc = 0.0;
+    CL_TRY(xy_inverse(ctx, pe, epi, ws.S));
+    if (rescale) {
+      count_small();
+      k_finish_rl_scale<<<1, 256, 0, st>>>(ws.partial, P.xy_blocks, ws.dscal + 0,
+                                           ws.dscal + 1, sdev);
+      CL_CHECK(cudaGetLastError());
+    }
+  }
+  return Status::Ok();
+}
+
+Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
+              Dims kd, float* out, int iters) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  cudaStream_t st = ctx.exec_stream();
+  if (iters <= 0) {
+    // the reference leaves the output unwritten; return the input image
+    count_small();
+    k_copy<<<kReduceBlocks, 256, 0, st>>>(img, out, id.n());
+    CL_CHECK(cudaGetLastError());
+    return Status::Ok();
+  }
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  CL_TRY(rl_core(ctx, *pe, *ws, img, id, wd, iters, true));
+  count_small();
+  k_clip<<<kReduceBlocks, 256, 0, st>>>(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
+                                        ws->fscal);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
+                 Dims kd, float* out, int iters) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  cudaStream_t st = ctx.exec_stream();
+  if (iters <= 0) {
+    count_small();
+    k_copy<<<kReduceBlocks, 256, 0, st>>>(img, out, id.n());
+    CL_CHECK(cudaGetLastError());
+    return Status::Ok();
+  }
+  // h <- h / sum(h) (src/BlindMaximumLikelihoodDeconvolve.cxx:59)
+  count_small();
+  k_reduce_sum<<<kReduceBlocks, 256, 0, st>>>(ker, kd.n(), ws->partial);
+  count_small();
+  k_finish_inverse<<<1, 256, 0, st>>>(ws->partial, kReduceBlocks, ws->fscal + 2);
+  CL_CHECK(cudaGetLastError());
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, ws->fscal + 2));
+  CL_TRY(rl_core(ctx, *pe, *ws, img, id, wd, iters, false));
+  count_small();
+  k_clip<<<kReduceBlocks, 256, 0, st>>>(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
+                                        nullptr);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+// Jansen-van Cittert: the first update reads the padded image; every update
+// is a z pass (h * i) plus one fused XY pass (inverse, JVC update, store i',
+// forward transform of i' for the next update).
+Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
+               Dims kd, float* out, int iters, float /*image_max*/,
+               const float* /*smooth_sigma*/, int /*smooth_interval*/) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  const VolPlan& P = pe->P;
+  cudaStream_t st = ctx.exec_stream();
+  // A = max(unpadded image) / 2 (src/JansenVanCittertDeconvolve.cxx:324)
+  float* pmax = reinterpret_cast<float*>(ws->partial);
+  count_small();
+  k_reduce_max<<<kReduceBlocks, 256, 0, st>>>(img, id.n(), pmax);
+  count_small();
+  k_finish_jvc<<<1, 32, 0, st>>>(pmax, kReduceBlocks, ws->fscal + 4);
+  CL_CHECK(cudaGetLastError());
+  // A and invASq are needed as kernel arguments: read them back once.
+  float hc[2];
+  CL_CHECK(cudaMemcpyAsync(hc, ws->fscal + 4, sizeof(hc), cudaMemcpyDeviceToHost, st));
+  CL_CHECK(cudaStreamSynchronize(st));
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  const PaddedSrc g = padded(img, id, wd, 0, 0, 0);
+  const WorkVol wv{wd.x, wd.y, wd.z};
+  const float scale_n = inv_volume(wd);
+  const int total = iters > 1 ? iters : 1;
+  CL_TRY(xy_forward(ctx, *pe, ProPadded{g, nullptr, P.xmode}, ws->S));
+  for (int k = 0; k < total; ++k) {
+    CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, scale_n}, ws->S, ws->S));
+    EpiJVC epi{k == 0 ? nullptr : ws->u, g, ws->u, hc[0], hc[1], wv, P.xmode};
+    if (k + 1 < total)
+      CL_TRY(xy_inv_fwd(ctx, *pe, epi, ws->S));
+    else
+      CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
+  }
+  count_small();
+  k_clip<<<kReduceBlocks, 256, 0, st>>>(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
+                                        nullptr);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+Status run_idivergence(Context& ctx, const float* g, const float* ghat,
+                       long long n, double* result) {
+  cudaStream_t st = ctx.exec_stream();
+  double* part = nullptr;
+  double* d = nullptr;
+  CL_CHECK(dev_alloc((void**)&part, sizeof(double) * kReduceBlocks));
+  CL_CHECK(dev_alloc((void**)&d, sizeof(double)));
+  count_small();
+  k_idiv<<<kReduceBlocks, 256, 0, st>>>(g, ghat, n, part);
+  count_small();
+  k_finish_sum<<<1, 256, 0, st>>>(part, kReduceBlocks, d);
+  cudaError_t e = cudaMemcpyAsync(result, d, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(part);
+  cudaFree(d);
+  CL_CHECK(e);
+  return Status::Ok();
+}
+
+}  // namespace clarity

@@ -1,0 +1,123 @@
+// engine.hpp -- internal C++ interface between the C ABI layer and the CUDA
+// engine.  Everything here works on DEVICE pointers and enqueues on the
+// context stream; the C ABI layer owns host<->device staging.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/clarity.h"
+#include "plan.hpp"
+
+namespace clarity {
+
+struct Dims {
+  int x, y, z;
+  long long n() const { return (long long)x * y * z; }
+};
+
+// Error with a ClarityResult_t code and a message for clarityx_last_error.
+struct Status {
+  ClarityResult_t code = CLARITY_SUCCESS;
+  std::string msg;
+  bool ok() const { return code == CLARITY_SUCCESS; }
+  static Status Ok() { return Status(); }
+};
+
+Status status_from_cuda(cudaError_t e, const char* what);
+
+// Plans are built once per work box and cached; tables live on the device.
+struct PlanEntry {
+  VolPlan P;
+  float2* tw = nullptr;  // twiddle tables (FP64-generated, rounded)
+  int* xrev = nullptr;   // natural x frequency -> smem slot after x passes
+};
+
+// Planner (host only).  Returns false for shapes it cannot decompose.
+bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why);
+
+// Device allocation that honours the host-side fault injector.
+cudaError_t dev_alloc(void** p, size_t bytes);
+void set_alloc_failure_countdown(int n);
+
+// Reusable device buffers for one work box.
+struct Workspace {
+  float2* S = nullptr;     // work spectrum (S layout)
+  float2* H = nullptr;     // OTF (S layout)
+  float* u = nullptr;      // work-box real volume (estimate)
+  float* img = nullptr;    // unpadded image
+  float* ker = nullptr;    // unpadded kernel
+  double* partial = nullptr;
+  double* dscal = nullptr; // [0] energy, [1] last sum, [2..] misc
+  float* fscal = nullptr;  // [0] deferred scale, [1] ones, [2..] misc
+  size_t img_cap = 0, ker_cap = 0;
+  long long spec_cap = 0, work_cap = 0;
+  int partial_cap = 0;
+};
+
+class Context {
+ public:
+  explicit Context(int device);
+  ~Context();
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+  void set_stream(cudaStream_t s) { user_stream_ = s; }
+  cudaStream_t exec_stream() const { return user_stream_ ? user_stream_ : stream_; }
+
+  Status plan(const Dims& work, const PlanEntry** out);
+  Status workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
+                   Workspace** out);
+  void release_workspaces();
+
+  std::mutex mu;  // serialises API calls on this context
+
+ private:
+  int device_;
+  cudaStream_t stream_ = nullptr;
+  cudaStream_t user_stream_ = nullptr;
+  std::map<std::tuple<int, int, int>, std::unique_ptr<PlanEntry>> plans_;
+  Workspace ws_;
+};
+
+// ----------------------------------------------------------- algorithms
+// All take unpadded device volumes and write the clipped result to a device
+// buffer of imageDim voxels.  They enqueue on ctx.exec_stream() only.
+Status run_convolve(Context& ctx, const float* img, Dims id, const float* ker,
+                    Dims kd, float* out);
+Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
+                  Dims kd, float* out, float eps);
+Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
+              Dims kd, float* out, int iters);
+Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
+                 Dims kd, float* out, int iters);
+Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
+               Dims kd, float* out, int iters, float image_max,
+               const float* smooth_sigma, int smooth_interval);
+// FP64 I-divergence of g against ghat (both unpadded device volumes).
+Status run_idivergence(Context& ctx, const float* g, const float* ghat,
+                       long long n, double* result);
+
+Context* global_context();  // nullptr when not registered
+
+// ------------------------------------------------ launch accounting
+// Kernel families timed by the optional event probes.
+enum KernelKind { KK_XY_FORWARD = 0, KK_Z = 1, KK_XY_INV_FWD = 2, KK_XY_INVERSE = 3,
+                  KK_OTHER = 4, KK_COUNT = 5 };
+// Counts every kernel launch of the library (for benchmarks) and, when
+// timing is enabled, records a CUDA event pair around each fused-pass launch
+// on the launching stream.
+void note_launch_begin(int kind, cudaStream_t st);
+void note_launch_end(int kind, cudaStream_t st);
+long long launch_count();
+void timing_enable(bool on);
+// Synchronises the recorded events and returns per-kind totals (ms) and
+// counts; clears the record.
+void timing_collect(double* ms, long long* counts);
+
+}  // namespace clarity

@@ -1,0 +1,7 @@
+// kern_xy_fwd.cu -- explicit instantiations of the fused pass kernels (see launch.cuh).
+#include "launch.cuh"
+
+namespace clarity {
+template Status xy_forward<ProWork>(Context&, const PlanEntry&, const ProWork&, float2*);
+template Status xy_forward<ProPadded>(Context&, const PlanEntry&, const ProPadded&, float2*);
+}  // namespace clarity

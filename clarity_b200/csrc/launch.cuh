@@ -1,0 +1,110 @@
+// launch.cuh -- host-side launch wrappers of the fused pass kernels.  The
+// template bodies live here; each kern_*.cu file instantiates one family so
+// the heavy kernels compile in parallel, and engine.cu sees them through the
+// extern declarations at the bottom.
+#pragma once
+#include "engine.hpp"
+#include "ops.cuh"
+#include "passes.cuh"
+
+namespace clarity {
+
+#ifndef CL_CHECK
+#define CL_CHECK(call)                                         \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return status_from_cuda(e_, #call); \
+  } while (0)
+#endif
+
+template <class K>
+static cudaError_t prep_kernel(K kernel, int smem) {
+  // Opt in to the dynamic shared memory this launch needs (idempotent).
+  if (smem > 48 * 1024)
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem);
+  return cudaSuccess;
+}
+
+template <class Pro>
+Status xy_forward(Context& ctx, const PlanEntry& pe, const Pro& pro,
+                         float2* S) {
+  const VolPlan& P = pe.P;
+  auto k = k_xy_forward<Pro>;
+  CL_CHECK(prep_kernel(k, P.xy_smem));
+  note_launch_begin(KK_XY_FORWARD, ctx.exec_stream());
+  k<<<P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream()>>>(P, pro, S, pe.tw,
+                                                                 pe.xrev);
+  note_launch_end(KK_XY_FORWARD, ctx.exec_stream());
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+template <class Epi>
+Status xy_inverse(Context& ctx, const PlanEntry& pe, const Epi& epi,
+                         const float2* S) {
+  const VolPlan& P = pe.P;
+  auto k = k_xy_inverse<Epi>;
+  CL_CHECK(prep_kernel(k, P.xy_smem));
+  note_launch_begin(KK_XY_INVERSE, ctx.exec_stream());
+  k<<<P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream()>>>(P, epi, S, pe.tw,
+                                                                 pe.xrev);
+  note_launch_end(KK_XY_INVERSE, ctx.exec_stream());
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+template <class Mid>
+Status xy_inv_fwd(Context& ctx, const PlanEntry& pe, const Mid& mid,
+                         float2* S) {
+  const VolPlan& P = pe.P;
+  auto k = k_xy_inv_fwd<Mid>;
+  CL_CHECK(prep_kernel(k, P.xy_smem));
+  note_launch_begin(KK_XY_INV_FWD, ctx.exec_stream());
+  k<<<P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream()>>>(P, mid, S, pe.tw,
+                                                                 pe.xrev);
+  note_launch_end(KK_XY_INV_FWD, ctx.exec_stream());
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+template <class Mod>
+Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
+                     const float2* Sin, float2* Sout) {
+  const VolPlan& P = pe.P;
+  auto k = k_z<Mod>;
+  CL_CHECK(prep_kernel(k, P.z_smem));
+  note_launch_begin(KK_Z, ctx.exec_stream());
+  k<<<P.z_blocks, P.z_threads, P.z_smem, ctx.exec_stream()>>>(P, mod, Sin, Sout,
+                                                              pe.tw);
+  note_launch_end(KK_Z, ctx.exec_stream());
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+
+#define CLARITY_EXTERN_LAUNCHES                                                     \
+  extern template Status xy_forward<ProWork>(Context&, const PlanEntry&,            \
+                                             const ProWork&, float2*);              \
+  extern template Status xy_forward<ProPadded>(Context&, const PlanEntry&,          \
+                                               const ProPadded&, float2*);          \
+  extern template Status xy_inverse<EpiClip>(Context&, const PlanEntry&,            \
+                                             const EpiClip&, const float2*);        \
+  extern template Status xy_inverse<EpiWork>(Context&, const PlanEntry&,            \
+                                             const EpiWork&, const float2*);        \
+  extern template Status xy_inverse<EpiRLProduct>(Context&, const PlanEntry&,       \
+                                                  const EpiRLProduct&, const float2*); \
+  extern template Status xy_inverse<EpiJVC>(Context&, const PlanEntry&,             \
+                                            const EpiJVC&, const float2*);          \
+  extern template Status xy_inv_fwd<MidRLRatio>(Context&, const PlanEntry&,         \
+                                                const MidRLRatio&, float2*);        \
+  extern template Status xy_inv_fwd<EpiJVC>(Context&, const PlanEntry&,             \
+                                            const EpiJVC&, float2*);                \
+  extern template Status z_pass<ModOTF>(Context&, const PlanEntry&, const ModOTF&,  \
+                                        const float2*, float2*);                    \
+  extern template Status z_pass<ModWiener>(Context&, const PlanEntry&,              \
+                                           const ModWiener&, const float2*, float2*); \
+  extern template Status z_pass<ModForward>(Context&, const PlanEntry&,             \
+                                            const ModForward&, const float2*, float2*);
+
+}  // namespace clarity

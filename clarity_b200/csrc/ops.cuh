@@ -1,0 +1,279 @@
+// ops.cuh -- operations fused into the FFT passes.
+//
+// Prologues (XY forward): load_c(m, y, z) returns complex row element m of
+//   row (y, z): (v[2m], v[2m+1]) for even nx, (v[m], 0) for odd nx.
+// Epilogues (XY inverse): apply_c(m, y, z, c) receives the same pair of
+//   real-space values after the inverse transform; the returned pair feeds
+//   the forward transform when the epilogue is fused into k_xy_inv_fwd.
+// Spectral operations (Z pass): apply(idx, v) with idx the element's offset
+//   in the S layout (the OTF shares that layout).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "dft_codelets.cuh"
+#include "plan.hpp"
+
+namespace clarity {
+
+// The reference divide of src/ComputePrimitives.cxx:144-148 (and
+// ComputePrimitivesGPU.cu:180-184) tests fabs(b) < 1e-5 in double; for a
+// float b that is exactly fabsf(b) <= 1e-5f (1e-5f is the largest float
+// below 1e-5).
+__device__ __forceinline__ float rl_ratio(float g, float b) {
+  return (fabsf(b) <= 1e-5f) ? 0.f : g / b;
+}
+
+// Real volume on the padded work box, x fastest.
+struct WorkVol {
+  int nx, ny, nz;
+  __device__ __forceinline__ long long idx(int x, int y, int z) const {
+    return ((long long)z * ny + y) * nx + x;
+  }
+};
+
+// Source volume of size (X, Y, Z) seen on the work box through the
+// reference's cyclic pad/shift (src/ImagePadSpatialShift.cxx:42-66):
+// work coordinate d maps to s = ((d - shift) wrapped) % dim, inside when
+// s < src dim, otherwise the fill value (0).
+struct PaddedSrc {
+  const float* __restrict__ src;
+  int X, Y, Z;       // source dims
+  int sx, sy, sz;    // shift
+  int nx, ny, nz;    // work dims
+  __device__ __forceinline__ static int wrap(int d, int shift, int n) {
+    int s = d - shift;
+    if (s < 0) s += n;
+    return s % n;
+  }
+  __device__ __forceinline__ float at(int x, int y, int z) const {
+    const int k = wrap(z, sz, nz);
+    const int j = wrap(y, sy, ny);
+    const int i = wrap(x, sx, nx);
+    if (i >= 0 && j >= 0 && k >= 0 && i < X && j < Y && k < Z)
+      return __ldg(&src[((long long)k * Y + j) * X + i]);
+    return 0.f;
+  }
+};
+
+// ---------------------------------------------------------------- prologues
+// Plain work-box volume, optionally multiplied by a device-resident scale
+// (the deferred RL flux rescale).
+struct ProWork {
+  const float* __restrict__ v;
+  const float* __restrict__ scale;  // nullptr -> 1
+  WorkVol w;
+  int xmode;
+  __device__ __forceinline__ float2 load_c(int m, int y, int z) const {
+    const float s = scale ? *scale : 1.f;
+    if (xmode == 0) {
+      const float2 a = __ldg(reinterpret_cast<const float2*>(v + w.idx(2 * m, y, z)));
+      return scale ? make_float2(s * a.x, s * a.y) : a;
+    }
+    const float a = __ldg(&v[w.idx(m, y, z)]);
+    return make_float2(scale ? s * a : a, 0.f);
+  }
+  __device__ __forceinline__ void finish() const {}
+};
+
+// Unpadded source read through the pad/shift map, times an optional scale.
+struct ProPadded {
+  PaddedSrc p;
+  const float* __restrict__ scale;  // nullptr -> 1
+  int xmode;
+  __device__ __forceinline__ float2 load_c(int m, int y, int z) const {
+    const float s = scale ? *scale : 1.f;
+    if (xmode == 0) {
+      float a = p.at(2 * m, y, z), b = p.at(2 * m + 1, y, z);
+      if (scale) { a = s * a; b = s * b; }
+      return make_float2(a, b);
+    }
+    float a = p.at(m, y, z);
+    if (scale) a = s * a;
+    return make_float2(a, 0.f);
+  }
+  __device__ __forceinline__ void finish() const {}
+};
+
+// ---------------------------------------------------------------- epilogues
+// Block-wide FP64 sum of per-thread partials into partial[blockIdx.x]
+// (fixed reduction order: deterministic).
+__device__ __forceinline__ void block_sum_store(double acc, double* partial) {
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double a = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) partial[blockIdx.x] = a;
+  }
+}
+
+// Store the real-space result on the work box.
+struct EpiWork {
+  float* __restrict__ out;
+  WorkVol w;
+  int xmode;
+  __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 c) {
+    if (xmode == 0)
+      *reinterpret_cast<float2*>(out + w.idx(2 * m, y, z)) = c;
+    else
+      out[w.idx(m, y, z)] = c.x;
+    return c;
+  }
+  __device__ __forceinline__ void finish() {}
+};
+
+// Store only the image region (crop from the origin, src/ImageClip.cxx:41-46)
+// into an unpadded (X, Y, Z) volume, times an optional device scale.
+struct EpiClip {
+  float* __restrict__ out;
+  int X, Y, Z;
+  const float* __restrict__ scale;
+  int xmode;
+  __device__ __forceinline__ void put(int x, int y, int z, float v) {
+    if (x < X && y < Y && z < Z) {
+      if (scale) v = *scale * v;
+      out[((long long)z * Y + y) * X + x] = v;
+    }
+  }
+  __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 c) {
+    if (xmode == 0) {
+      put(2 * m, y, z, c.x);
+      put(2 * m + 1, y, z, c.y);
+    } else {
+      put(m, y, z, c.x);
+    }
+    return c;
+  }
+  __device__ __forceinline__ void finish() {}
+};
+
+// RL step 4 (src/MaximumLikelihoodDeconvolve.cxx:69-70) with the flux sum of
+// step 5 (:73-74): u_new = cur * c, cur = scale * u (or the padded image on
+// the first iteration), partial sums of u_new in FP64.
+struct EpiRLProduct {
+  const float* __restrict__ cur;     // work-box estimate, or nullptr
+  PaddedSrc g;                       // used when cur == nullptr
+  const float* __restrict__ scale;   // deferred flux scale for cur
+  float* __restrict__ unew;
+  double* __restrict__ partial;
+  WorkVol w;
+  int xmode;
+  double acc;
+  __device__ __forceinline__ float cur_at(int x, int y, int z) const {
+    if (cur) {
+      const float u = __ldg(&cur[w.idx(x, y, z)]);
+      return scale ? *scale * u : u;
+    }
+    return g.at(x, y, z);
+  }
+  __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 c) {
+    if (xmode == 0) {
+      const float a = cur_at(2 * m, y, z) * c.x;
+      const float b = cur_at(2 * m + 1, y, z) * c.y;
+      *reinterpret_cast<float2*>(unew + w.idx(2 * m, y, z)) = make_float2(a, b);
+      acc += (double)a;
+      acc += (double)b;
+      return make_float2(a, b);
+    }
+    const float a = cur_at(m, y, z) * c.x;
+    unew[w.idx(m, y, z)] = a;
+    acc += (double)a;
+    return make_float2(a, 0.f);
+  }
+  __device__ __forceinline__ void finish() { block_sum_store(acc, partial); }
+};
+
+// RL step 2 (src/MaximumLikelihoodDeconvolve.cxx:61-62): r = g / (h*u) with
+// the 1e-5 guard, fused between the inverse and forward transforms.
+struct MidRLRatio {
+  PaddedSrc g;
+  int xmode;
+  __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 b) {
+    if (xmode == 0)
+      return make_float2(rl_ratio(g.at(2 * m, y, z), b.x),
+                         rl_ratio(g.at(2 * m + 1, y, z), b.y));
+    return make_float2(rl_ratio(g.at(m, y, z), b.x), 0.f);
+  }
+  __device__ __forceinline__ void finish() {}
+};
+
+// JVC update (src/JansenVanCittertDeconvolve.cxx:106-111,
+// JansenVanCittertDeconvolveGPU.cu:43-49): i' = max(0, i + gamma(o) (g - o)),
+// gamma(o) = 1 - (o - A)^2 / A^2.  cur == nullptr reads i from the padded
+// image (first update).  Stores i' on the work box and returns it, so the
+// fused kernel transforms it for the next iteration.
+struct EpiJVC {
+  const float* __restrict__ cur;
+  PaddedSrc g;
+  float* __restrict__ inext;
+  float A, invASq;
+  WorkVol w;
+  int xmode;
+  __device__ __forceinline__ float upd(float i, float gv, float o) const {
+    const float diff = o - A;
+    const float gamma = 1.0f - ((diff * diff) * invASq);
+    const float val = i + (gamma * (gv - o));
+    return val < 0.0f ? 0.0f : val;
+  }
+  __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 o) {
+    if (xmode == 0) {
+      const int x = 2 * m;
+      const float g0 = g.at(x, y, z), g1 = g.at(x + 1, y, z);
+      const float i0 = cur ? __ldg(&cur[w.idx(x, y, z)]) : g0;
+      const float i1 = cur ? __ldg(&cur[w.idx(x + 1, y, z)]) : g1;
+      const float2 r = make_float2(upd(i0, g0, o.x), upd(i1, g1, o.y));
+      *reinterpret_cast<float2*>(inext + w.idx(x, y, z)) = r;
+      return r;
+    }
+    const float g0 = g.at(m, y, z);
+    const float i0 = cur ? __ldg(&cur[w.idx(m, y, z)]) : g0;
+    const float r = upd(i0, g0, o.x);
+    inext[w.idx(m, y, z)] = r;
+    return make_float2(r, 0.f);
+  }
+  __device__ __forceinline__ void finish() {}
+};
+
+// ------------------------------------------------------------ spectral ops
+// src/ModulateGPU.cu:63-72 / Convolve.cxx:195-205: out = scale * (a * b),
+// no conjugate, a = data, b = OTF; the arithmetic order of
+// ComplexMultiplyAndScale (include/internal/Complex.h:95-102) is kept.
+struct ModOTF {
+  static constexpr bool forward_only = false;
+  const float2* __restrict__ H;
+  float scale;
+  __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
+    const float2 h = __ldg(&H[idx]);
+    return make_float2(scale * (v.x * h.x - v.y * h.y),
+                       scale * (v.x * h.y + v.y * h.x));
+  }
+};
+
+// src/WienerDeconvolveGPU.cu:43-49: conj(H) / (|H|^2 + eps), then
+// scale * (that * G).
+struct ModWiener {
+  static constexpr bool forward_only = false;
+  const float2* __restrict__ H;
+  float eps, scale;
+  __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
+    const float2 h = __ldg(&H[idx]);
+    const float mag = h.x * h.x + h.y * h.y;
+    const float f = 1.0f / (mag + eps);
+    const float a = h.x * f, b = -h.y * f;
+    return make_float2(scale * (a * v.x - b * v.y), scale * (a * v.y + b * v.x));
+  }
+};
+
+struct ModForward {
+  static constexpr bool forward_only = true;
+  __device__ __forceinline__ float2 apply(long long, float2 v) const { return v; }
+};
+
+}  // namespace clarity

@@ -1,0 +1,73 @@
+// plan.hpp -- FFT plan for one padded work box (nx, ny, nz).
+//
+// The 3-D real transform the reference takes with FFTW/cuFFT on every call
+// (src/FFT.cxx:46-146: unnormalised r2c with x halved, c2r back) is split
+// into two fused passes over HBM:
+//
+//   XY pass  one thread block per (z, group of G consecutive y0):
+//            x r2c of the G*Ay rows y = y0 + By*j (j < Ay) in shared memory,
+//            then the length-Ay DFT over j and the twiddle w_ny^(y0*k1)
+//            (four-step split of the y axis, ny = Ay*By).
+//   Z pass   one thread block per (k1, group of W x-frequencies): the
+//            length-By DFT over y0 and the full z DFT, the spectral
+//            operation (OTF multiply, Wiener filter, ...), then the inverse
+//            z and By transforms, all in shared memory.
+//
+// Spectrum layout in HBM ("S layout", complex float):
+//   S[k1][kg][z][y0][ki]   k1 < Ay, kg < KG, z < nz, y0 < By, ki < W,
+//   with x-frequency kx = kg*W + ki (natural order, kx < XS <= KG*W).
+// A Z-pass tile S[k1][kg] is one contiguous block of nz*By*W elements.  The
+// order of the y0 and z frequencies inside a tile is the digit-reversed
+// order the in-place register passes leave; it never leaves the library and
+// the OTF is produced by the same passes, so products line up.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace clarity {
+
+constexpr int kMaxPasses = 4;
+
+// One complex DFT length n as register passes in decimation-in-frequency
+// order.  Pass s works on sub-transforms of length len[s]; a register line
+// of pass s holds radix[s] elements spaced span[s] = len[s]/radix[s] apart.
+struct AxisPlan {
+  int n;
+  int npass;
+  int radix[kMaxPasses];
+  int len[kMaxPasses];
+  int span[kMaxPasses];
+  int tw_off;  // offset of the w_n^t (t < n) table in the twiddle buffer
+};
+
+struct VolPlan {
+  int nx, ny, nz;
+  int xmode;   // 0: nx even (half-length complex + r2c split); 1: nx odd
+  int M;       // complex row length in the XY pass (nx/2 or nx)
+  int XS;      // x-frequency slots (M+1 or nx)
+  int items;   // r2c work items per row group (pairs k, M-k)
+  int Ay, By;  // ny = Ay * By
+  int G;       // y0 values per XY tile (divides By)
+  int W;       // x-frequency slots per Z tile
+  int KG;      // ceil(XS / W)
+  int rowStride;  // float2 per row in XY shared memory (padded)
+  int padShift;   // XY smem index p -> p + (p >> padShift)
+  AxisPlan ax;    // length M
+  AxisPlan ayB;   // length By
+  AxisPlan az;    // length nz
+  int tw_r2c_off;   // w_nx^k, k <= M/2          (even mode)
+  int tw_ny_off;    // w_ny^t, t < ny            (y split twiddle)
+  int xrev_off;     // int table: natural k -> smem slot after x passes
+  int twiddle_count;  // float2 entries in the twiddle buffer
+  int xrev_count;
+  long long spec_elems;  // Ay*KG*nz*By*W
+  int xy_blocks, z_blocks;
+  int xy_threads, z_threads;
+  int xy_smem, z_smem;   // bytes of dynamic shared memory
+  long long n_real() const { return (long long)nx * ny * nz; }
+};
+
+// Radices accepted for one register pass (must match dft_codelets.cuh).
+constexpr int kRadixSet[] = {16, 19, 17, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+
+}  // namespace clarity

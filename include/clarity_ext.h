@@ -1,0 +1,78 @@
+/*
+ * clarity_ext.h -- extensions of the Clarity C ABI (no counterpart in the
+ * reference's public header).  Device-pointer entry points let a caller keep
+ * volumes resident in HBM across calls (the public Clarity_* functions take
+ * host buffers and copy in and out on every call); the rest are diagnostics
+ * and host-side fault injection for tests.
+ *
+ * Device-pointer functions: every pointer is a CUDA device pointer on the
+ * library's device; `stream` is a cudaStream_t (NULL = the library's own
+ * stream).  They are asynchronous with respect to the host unless stated.
+ */
+#ifndef CLARITY_B200_CLARITY_EXT_H_
+#define CLARITY_B200_CLARITY_EXT_H_
+
+#include "clarity.h"
+
+/* Message of the last failing call on this thread's library state, or "". */
+CLARITY_API const char *clarityx_last_error(void);
+
+/* CUDA device used by the next Clarity_Register that creates the context
+ * (default 0).  Returns CLARITY_INVALID_OPERATION once registered. */
+CLARITY_API ClarityResult_t clarityx_set_device(int device);
+
+/* Host-side fault injection for tests: the countdown-th device allocation
+ * from now fails as if cudaMalloc had run out of memory (0 disables). */
+CLARITY_API void clarityx_inject_device_alloc_failure(int countdown);
+
+/* Releases cached work buffers (plans stay cached). */
+CLARITY_API ClarityResult_t clarityx_trim(void);
+
+/* Blocks until all work the library enqueued has finished; returns the
+ * first asynchronous error as a result code. */
+CLARITY_API ClarityResult_t clarityx_synchronize(void *stream);
+
+/* Device-resident versions of the public algorithms.  image/kernel/out are
+ * unpadded device volumes of imageDim / kernelDim / imageDim voxels. */
+CLARITY_API ClarityResult_t clarityx_convolve_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, void *stream);
+CLARITY_API ClarityResult_t clarityx_wiener_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, float epsilon, void *stream);
+CLARITY_API ClarityResult_t clarityx_ml_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+CLARITY_API ClarityResult_t clarityx_blind_ml_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+CLARITY_API ClarityResult_t clarityx_jvc_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+
+/* I-divergence sum_i g ln(g/ghat) + ghat - g (alpha = 0 form of
+ * src/IDivergenceDeconvolve.cxx:33-47), accumulated in FP64; 0 ln 0 = 0 and
+ * voxels with g > 0 and ghat <= 0 are skipped.  Host buffers; synchronous. */
+CLARITY_API ClarityResult_t clarityx_idivergence(const float *g,
+                                                 const float *ghat,
+                                                 long long n, double *result);
+
+/* Plan chosen for a padded work box: fills up to 16 ints
+ * {M, XS, Ay, By, G, W, KG, xy_blocks, z_blocks, xy_smem, z_smem,
+ *  x passes, y0 passes, z passes, xmode, spec_elems / 1024}.
+ * Returns CLARITY_INVALID_ARGUMENT for shapes the planner rejects.  Needs
+ * no device. */
+CLARITY_API ClarityResult_t clarityx_plan_info(Clarity_Dim3 workDim,
+                                               int *fields, int nfields);
+
+/* Benchmark probes.  clarityx_launch_count: kernels the library has
+ * launched so far.  clarityx_timing_enable(1) makes every fused-pass launch
+ * record a CUDA event pair on its stream; clarityx_timing_collect waits for
+ * them and returns, per kernel family (0 xy-forward, 1 z, 2 xy-inverse+forward,
+ * 3 xy-inverse, 4 other), the summed milliseconds and launch counts, then
+ * clears the record. */
+CLARITY_API long long clarityx_launch_count(void);
+CLARITY_API void clarityx_timing_enable(int on);
+CLARITY_API void clarityx_timing_collect(double *ms, long long *counts, int n);
+
+#endif /* CLARITY_B200_CLARITY_EXT_H_ */

@@ -1,0 +1,402 @@
+// clarity_oracle.cpp -- TEST INFRASTRUCTURE ONLY (oracle).
+//
+// CPU restatement of the reference deconvolution path, used as the parity
+// checker for the CUDA library.  Only tests/, __graft_entry__.smoke() and
+// bench.py's CPU-baseline leg load it.  Every algorithm is templated on the
+// arithmetic type T (float reproduces the reference's FFTW float path; double
+// is the FP64 oracle every result's error is stated against) and follows the
+// cited reference lines step by step.  FFTs come from cpu_fft.hpp, a
+// restatement of FFTW's published transform definitions.
+//
+// Sum modes for the RL flux rescale (src/MaximumLikelihoodDeconvolve.cxx:73-78):
+//   SUM_SERIAL_T  serial accumulation in T, as Clarity_ReduceSum's CPU branch
+//                 (src/ComputePrimitives.cxx:61-71)
+//   SUM_DOUBLE    accumulation in double, rounded to T once (the parity
+//                 target; the CUDA library sums in FP64)
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "cpu_fft.hpp"
+
+namespace {
+
+enum { SUM_SERIAL_T = 0, SUM_DOUBLE = 1 };
+
+struct Dim3 {
+  int x, y, z;
+  long n() const { return (long)x * y * z; }
+};
+
+// src/ImagePadSpatialShift.cxx:32-69: dst[d] = src[(d - shift) mod dstDim]
+// when that index lies inside src, else fill.
+template <class T, class S>
+void pad_shift(T* dst, Dim3 dd, const S* src, Dim3 sd, const int shift[3],
+               T fill) {
+  for (int dk = 0; dk < dd.z; dk++) {
+    int sk = dk - shift[2];
+    if (sk < 0) sk += dd.z;
+    sk = sk % dd.z;
+    bool wk = sk >= 0 && sk < sd.z;
+    for (int dj = 0; dj < dd.y; dj++) {
+      int sj = dj - shift[1];
+      if (sj < 0) sj += dd.y;
+      sj = sj % dd.y;
+      bool wj = sj >= 0 && sj < sd.y;
+      for (int di = 0; di < dd.x; di++) {
+        int si = di - shift[0];
+        if (si < 0) si += dd.x;
+        si = si % dd.x;
+        bool wi = si >= 0 && si < sd.x;
+        long d = ((long)dk * dd.y + dj) * dd.x + di;
+        if (wi && wj && wk)
+          dst[d] = (T)src[((long)sk * sd.y + sj) * sd.x + si];
+        else
+          dst[d] = fill;
+      }
+    }
+  }
+}
+
+// src/ImageClip.cxx:30-50: crop from the origin.
+template <class T, class D>
+void clip(D* dst, Dim3 dd, const T* src, Dim3 sd) {
+  for (int k = 0; k < dd.z; k++)
+    for (int j = 0; j < dd.y; j++)
+      for (int i = 0; i < dd.x; i++)
+        dst[((long)k * dd.y + j) * dd.x + i] =
+            (D)src[((long)k * sd.y + j) * sd.x + i];
+}
+
+template <class T>
+struct Work {
+  Dim3 img, ker, wd;
+  long n, nc;
+  std::vector<T> g, h;  // padded image, padded+shifted kernel
+  template <class S>
+  Work(const S* in, Dim3 id, const S* kernel, Dim3 kd) : img(id), ker(kd) {
+    // src/MaximumLikelihoodDeconvolve.cxx:271-292 (same in every algorithm):
+    // work = image + kernel; image padded with zero shift, kernel shifted by
+    // -kernelDim/2 (truncating division) so its centre sits at the origin.
+    wd = Dim3{id.x + kd.x, id.y + kd.y, id.z + kd.z};
+    n = wd.n();
+    nc = (long)wd.z * wd.y * (wd.x / 2 + 1);
+    g.resize(n);
+    h.resize(n);
+    const int zero[3] = {0, 0, 0};
+    const int ks[3] = {-kd.x / 2, -kd.y / 2, -kd.z / 2};
+    pad_shift<T, S>(g.data(), wd, in, id, zero, (T)0);
+    pad_shift<T, S>(h.data(), wd, kernel, kd, ks, (T)0);
+  }
+  void r2c(const T* in, oracle::cx<T>* out) const {
+    oracle::r2c_3d<T>(wd.z, wd.y, wd.x, in, out);
+  }
+  void c2r(const oracle::cx<T>* in, T* out) const {
+    oracle::c2r_3d<T>(wd.z, wd.y, wd.x, in, out);
+  }
+};
+
+// src/Convolve.cxx:195-205 / include/internal/Complex.h:95-102:
+// out = scale * (a * b), complex multiply without conjugation.
+template <class T>
+void modulate(long nc, const oracle::cx<T>* a, const oracle::cx<T>* b,
+              T scale, oracle::cx<T>* out) {
+  for (long i = 0; i < nc; i++) {
+    T ar = a[i].real(), ai = a[i].imag(), br = b[i].real(), bi = b[i].imag();
+    out[i] = oracle::cx<T>(scale * (ar * br - ai * bi),
+                           scale * (ar * bi + ai * br));
+  }
+}
+
+template <class T>
+T inv_n(const Dim3& wd) {
+  // src/Convolve.cxx:199: 1.0f / ((float) nz*ny*nx)
+  return (T)1 / ((T)wd.z * wd.y * wd.x);
+}
+
+// src/Convolve.cxx:118-143: out = C2R(R2C(in) * otf / N)
+template <class T>
+void convolve_otf(const Work<T>& w, const T* in, const oracle::cx<T>* otf,
+                  T* out, std::vector<oracle::cx<T>>& tmp) {
+  w.r2c(in, tmp.data());
+  modulate<T>(w.nc, tmp.data(), otf, inv_n<T>(w.wd), tmp.data());
+  w.c2r(tmp.data(), out);
+}
+
+template <class T>
+T reduce_sum(const T* a, long n, int mode) {
+  if (mode == SUM_SERIAL_T) {
+    T s = 0;
+    for (long i = 0; i < n; i++) s += a[i];
+    return s;
+  }
+  double s = 0;
+  for (long i = 0; i < n; i++) s += (double)a[i];
+  return (T)s;
+}
+
+// Clarity_Convolve: src/Convolve.cxx:41-115,146-184.
+template <class T, class S>
+void convolve(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out,
+              T* out_work) {
+  Work<T> w(in, id, kernel, kd);
+  std::vector<oracle::cx<T>> a(w.nc), b(w.nc);
+  std::vector<T> o(w.n);
+  w.r2c(w.g.data(), a.data());
+  w.r2c(w.h.data(), b.data());
+  modulate<T>(w.nc, a.data(), b.data(), inv_n<T>(w.wd), a.data());
+  w.c2r(a.data(), o.data());
+  clip<T, S>(out, id, o.data(), w.wd);
+  if (out_work) std::memcpy(out_work, o.data(), sizeof(T) * w.n);
+}
+
+// Richardson-Lucy / ML: src/MaximumLikelihoodDeconvolve.cxx:84-153 with the
+// update of :48-81.  The returned estimate is the last iterate; the reference
+// leaves the output unwritten when iterations == 0, here the padded input is
+// returned (the state RL starts from).
+template <class T, class S>
+void rl(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
+        int sum_mode, T* out_work) {
+  Work<T> w(in, id, kernel, kd);
+  const long n = w.n;
+  std::vector<oracle::cx<T>> otf(w.nc), tmp(w.nc);
+  w.r2c(w.h.data(), otf.data());                      // :98
+  std::vector<T> u(w.g), s1(n), s2(n);
+  const T energy = reduce_sum<T>(w.g.data(), n, sum_mode);  // :133
+  for (int k = 0; k < iters; k++) {
+    // :57 s1 = h * u (no conjugate)
+    convolve_otf<T>(w, u.data(), otf.data(), s1.data(), tmp);
+    // :62 s1 = g / s1 with |s1| < 1e-5 -> 0 (src/ComputePrimitives.cxx:144-148);
+    // the comparison is made in double, as fabs(float) < 1e-5 is in C++
+    for (long i = 0; i < n; i++)
+      s1[i] = ((double)std::fabs(s1[i]) < 1e-5) ? (T)0 : w.g[i] / s1[i];
+    // :65 s2 = h * s1
+    convolve_otf<T>(w, s1.data(), otf.data(), s2.data(), tmp);
+    // :69-70 u = u * s2
+    for (long i = 0; i < n; i++) u[i] = u[i] * s2[i];
+    // :73-78 flux rescale over the whole padded box
+    const T ne = reduce_sum<T>(u.data(), n, sum_mode);
+    const T scale = energy / ne;
+    for (long i = 0; i < n; i++) u[i] = scale * u[i];
+  }
+  clip<T, S>(out, id, u.data(), w.wd);
+  if (out_work) std::memcpy(out_work, u.data(), sizeof(T) * n);
+}
+
+// Wiener: src/WienerDeconvolve.cxx:69-122 with the kernel of :48-66.
+template <class T, class S>
+void wiener(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, T eps,
+            T* out_work) {
+  Work<T> w(in, id, kernel, kd);
+  std::vector<oracle::cx<T>> G(w.nc), H(w.nc);
+  std::vector<T> o(w.n);
+  w.r2c(w.g.data(), G.data());
+  w.r2c(w.h.data(), H.data());
+  const T scale = inv_n<T>(w.wd);
+  for (long i = 0; i < w.nc; i++) {
+    T hr = H[i].real(), hi = -H[i].imag();       // conj(H)
+    T mag = H[i].real() * H[i].real() + H[i].imag() * H[i].imag();
+    T f = (T)1 / (mag + eps);
+    hr *= f;
+    hi *= f;
+    T gr = G[i].real(), gi = G[i].imag();
+    G[i] = oracle::cx<T>(scale * (hr * gr - hi * gi),
+                         scale * (hr * gi + hi * gr));
+  }
+  w.c2r(G.data(), o.data());
+  clip<T, S>(out, id, o.data(), w.wd);
+  if (out_work) std::memcpy(out_work, o.data(), sizeof(T) * w.n);
+}
+
+// JVC: src/JansenVanCittertDeconvolve.cxx:122-192 with the update of
+// :90-119 and A = max(unpadded image)/2 (:128-129, :324).  iterations <= 1
+// performs exactly one update (:167-173).
+template <class T, class S>
+void jvc(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
+         T* out_work) {
+  Work<T> w(in, id, kernel, kd);
+  const long n = w.n;
+  T mx = (T)in[0];
+  for (long i = 0; i < id.n(); i++)
+    if ((T)in[i] > mx) mx = (T)in[i];
+  const T A = (T)0.5 * mx;
+  const T invASq = (T)1 / (A * A);
+  std::vector<oracle::cx<T>> otf(w.nc), tmp(w.nc);
+  w.r2c(w.h.data(), otf.data());
+  std::vector<T> i_k(w.g), o(n);
+  const int total = iters > 1 ? iters : 1;
+  for (int k = 0; k < total; k++) {
+    convolve_otf<T>(w, i_k.data(), otf.data(), o.data(), tmp);
+    for (long j = 0; j < n; j++) {
+      T diff = o[j] - A;
+      T gamma = (T)1 - ((diff * diff) * invASq);
+      T val = i_k[j] + (gamma * (w.g[j] - o[j]));
+      if (val < (T)0) val = (T)0;
+      i_k[j] = val;
+    }
+  }
+  clip<T, S>(out, id, i_k.data(), w.wd);
+  if (out_work) std::memcpy(out_work, i_k.data(), sizeof(T) * n);
+}
+
+// Blind ML, reference CPU semantics: src/BlindMaximumLikelihoodDeconvolve.cxx
+// :102-148 with the update of :50-99.  h is renormalised to unit sum at the
+// start of every update (:59, Clarity_NormalizeArray) but never updated
+// (:96 is disabled); the discarded third convolution (:89-93) has no effect
+// on the result and is skipped; there is no flux rescale.
+template <class T, class S>
+void blind(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
+           int sum_mode, T* out_work) {
+  Work<T> w(in, id, kernel, kd);
+  const long n = w.n;
+  std::vector<oracle::cx<T>> O(w.nc), Hk(w.nc), t1(w.nc);
+  std::vector<T> u(w.g), tmp(n);
+  const T scale = inv_n<T>(w.wd);
+  for (int k = 0; k < iters; k++) {
+    // src/ComputePrimitives.cxx:197-209: h = h * (1 / sum h)
+    const T sum = reduce_sum<T>(w.h.data(), n, sum_mode);
+    const T inv = (T)1 / sum;
+    for (long i = 0; i < n; i++) w.h[i] = inv * w.h[i];
+    w.r2c(u.data(), O.data());
+    w.r2c(w.h.data(), Hk.data());
+    modulate<T>(w.nc, O.data(), Hk.data(), scale, t1.data());
+    w.c2r(t1.data(), tmp.data());
+    for (long i = 0; i < n; i++)
+      tmp[i] = ((double)std::fabs(tmp[i]) < 1e-5) ? (T)0 : w.g[i] / tmp[i];
+    w.r2c(tmp.data(), t1.data());
+    modulate<T>(w.nc, t1.data(), Hk.data(), scale, t1.data());
+    w.c2r(t1.data(), tmp.data());
+    for (long i = 0; i < n; i++) u[i] = u[i] * tmp[i];
+  }
+  clip<T, S>(out, id, u.data(), w.wd);
+  if (out_work) std::memcpy(out_work, u.data(), sizeof(T) * n);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI ---
+// Volumes are x-fastest float arrays; *_f64 variants compute in double but
+// take and return float volumes (the padded work-box result, when requested
+// through out_work, is returned in the computing precision).
+extern "C" {
+
+#define ORACLE_DIMS                                                   \
+  Dim3 id{ix, iy, iz};                                                \
+  Dim3 kd{kx, ky, kz}
+
+void oracle_convolve_f32(const float* in, int ix, int iy, int iz,
+                         const float* k, int kx, int ky, int kz, float* out,
+                         float* work) {
+  ORACLE_DIMS;
+  convolve<float, float>(in, id, k, kd, out, work);
+}
+void oracle_convolve_f64(const float* in, int ix, int iy, int iz,
+                         const float* k, int kx, int ky, int kz, float* out,
+                         double* work) {
+  ORACLE_DIMS;
+  convolve<double, float>(in, id, k, kd, out, work);
+}
+void oracle_rl_f32(const float* in, int ix, int iy, int iz, const float* k,
+                   int kx, int ky, int kz, float* out, int iters,
+                   int sum_mode, float* work) {
+  ORACLE_DIMS;
+  rl<float, float>(in, id, k, kd, out, iters, sum_mode, work);
+}
+void oracle_rl_f64(const float* in, int ix, int iy, int iz, const float* k,
+                   int kx, int ky, int kz, float* out, int iters,
+                   double* work) {
+  ORACLE_DIMS;
+  rl<double, float>(in, id, k, kd, out, iters, SUM_DOUBLE, work);
+}
+void oracle_wiener_f32(const float* in, int ix, int iy, int iz,
+                       const float* k, int kx, int ky, int kz, float* out,
+                       float eps, float* work) {
+  ORACLE_DIMS;
+  wiener<float, float>(in, id, k, kd, out, eps, work);
+}
+void oracle_wiener_f64(const float* in, int ix, int iy, int iz,
+                       const float* k, int kx, int ky, int kz, float* out,
+                       double eps, double* work) {
+  ORACLE_DIMS;
+  wiener<double, float>(in, id, k, kd, out, eps, work);
+}
+void oracle_jvc_f32(const float* in, int ix, int iy, int iz, const float* k,
+                    int kx, int ky, int kz, float* out, int iters,
+                    float* work) {
+  ORACLE_DIMS;
+  jvc<float, float>(in, id, k, kd, out, iters, work);
+}
+void oracle_jvc_f64(const float* in, int ix, int iy, int iz, const float* k,
+                    int kx, int ky, int kz, float* out, int iters,
+                    double* work) {
+  ORACLE_DIMS;
+  jvc<double, float>(in, id, k, kd, out, iters, work);
+}
+void oracle_blind_f32(const float* in, int ix, int iy, int iz,
+                      const float* k, int kx, int ky, int kz, float* out,
+                      int iters, int sum_mode, float* work) {
+  ORACLE_DIMS;
+  blind<float, float>(in, id, k, kd, out, iters, sum_mode, work);
+}
+void oracle_blind_f64(const float* in, int ix, int iy, int iz,
+                      const float* k, int kx, int ky, int kz, float* out,
+                      int iters, double* work) {
+  ORACLE_DIMS;
+  blind<double, float>(in, id, k, kd, out, iters, SUM_DOUBLE, work);
+}
+
+// I-divergence of src/IDivergenceDeconvolve.cxx:33-47 with alpha = 0, in
+// double: sum over voxels with g > 0 of g ln(g / ghat) + ghat - g, plus ghat
+// where g == 0 (0 ln 0 = 0).  Voxels with ghat <= 0 and g > 0 are skipped
+// and counted in *skipped.
+double oracle_idivergence(const float* g, const float* ghat, long n,
+                          long* skipped) {
+  double s = 0;
+  long sk = 0;
+  for (long i = 0; i < n; i++) {
+    const double a = g[i], b = ghat[i];
+    if (a > 0) {
+      if (b <= 0) { sk++; continue; }
+      s += a * std::log(a / b) + b - a;
+    } else {
+      s += b - a;
+    }
+  }
+  if (skipped) *skipped = sk;
+  return s;
+}
+
+// Pad/shift and clip exactly as the reference public utilities.
+void oracle_pad_shift(float* dst, int dx, int dy, int dz, const float* src,
+                      int sx, int sy, int sz, const int shift[3], float fill) {
+  pad_shift<float, float>(dst, Dim3{dx, dy, dz}, src, Dim3{sx, sy, sz}, shift,
+                          fill);
+}
+
+// Raw 3-D transforms (FFTW layout) for checking the FFT restatement.
+void oracle_r2c_3d_f32(int nz, int ny, int nx, const float* in, float* out) {
+  oracle::r2c_3d<float>(nz, ny, nx, in,
+                        reinterpret_cast<std::complex<float>*>(out));
+}
+void oracle_c2r_3d_f32(int nz, int ny, int nx, const float* in, float* out) {
+  oracle::c2r_3d<float>(nz, ny, nx,
+                        reinterpret_cast<const std::complex<float>*>(in), out);
+}
+void oracle_r2c_3d_f64(int nz, int ny, int nx, const double* in, double* out) {
+  oracle::r2c_3d<double>(nz, ny, nx, in,
+                         reinterpret_cast<std::complex<double>*>(out));
+}
+void oracle_c2r_3d_f64(int nz, int ny, int nx, const double* in, double* out) {
+  oracle::c2r_3d<double>(nz, ny, nx,
+                         reinterpret_cast<const std::complex<double>*>(in),
+                         out);
+}
+
+void oracle_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : 1);
+#endif
+}
+
+}  // extern "C"

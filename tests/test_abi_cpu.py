@@ -1,0 +1,116 @@
+"""CPU tests of the C ABI library: it loads, exports every declared symbol,
+keeps the reference's result codes, and its host-side logic (argument
+checks, pad/clip utilities, planner) behaves without a GPU."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from clarity_b200 import api
+from conftest import ROOT, gpu_available
+
+HEADERS = [os.path.join(ROOT, "include", "clarity.h"),
+           os.path.join(ROOT, "include", "clarity_ext.h")]
+
+
+def declared_symbols():
+    names = []
+    for h in HEADERS:
+        text = open(h).read()
+        for m in re.finditer(r"^CLARITY_API\b[^;(]*?\b(\w+)\s*\(", text, re.S | re.M):
+            names.append(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = api.load()
+    names = declared_symbols()
+    assert set(api.PUBLIC_SYMBOLS) <= set(names)
+    assert set(api.EXTENSION_SYMBOLS) <= set(names)
+    out = subprocess.run(["nm", "-D", "--defined-only", api.LIB_PATH],
+                         capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    for n in names:
+        assert n in exported, n
+        getattr(lib, n)
+
+
+def test_result_codes_match_reference_enum_order():
+    # Clarity.h.in:90-101: FFT_FAILED=0 ... SUCCESS=5
+    text = open(HEADERS[0]).read()
+    for name, val in [("CLARITY_FFT_FAILED", 0), ("CLARITY_OUT_OF_MEMORY", 1),
+                      ("CLARITY_DEVICE_OUT_OF_MEMORY", 2), ("CLARITY_INVALID_OPERATION", 3),
+                      ("CLARITY_INVALID_ARGUMENT", 4), ("CLARITY_SUCCESS", 5)]:
+        assert re.search(rf"{name}\s*=\s*{val}\b", text)
+        assert getattr(api, name) == val
+        assert api.result_string(val) == name
+    assert api.result_string(17) == "<unknown Clarity result>"
+
+
+def test_dim3_from_array():
+    arr = (C.c_int * 3)(7, 8, 9)
+    d = api.load().Clarity_Dim3FromArray(arr)
+    assert (d.x, d.y, d.z) == (7, 8, 9)
+
+
+def test_pad_shift_and_clip_match_oracle(oracle_lib):
+    src = np.random.default_rng(4).random((3, 5, 7)).astype(np.float32)
+    for shift in [(0, 0, 0), (-3, -2, -1), (2, 1, 0), (-7, 5, -3)]:
+        ours = api.image_pad_spatial_shift(src, (6, 9, 11), shift, 0.25)
+        want = oracle_lib.pad_shift(src, (6, 9, 11), shift, 0.25)
+        assert np.array_equal(ours, want)
+    big = np.random.default_rng(5).random((6, 9, 11)).astype(np.float32)
+    assert np.array_equal(api.image_clip(big, (3, 5, 7)), big[:3, :5, :7])
+
+
+def test_argument_errors_without_device():
+    img = np.ones((4, 4, 4), np.float32)
+    L = api.load()
+    # NULL buffers -> CLARITY_INVALID_ARGUMENT (src/ImageClip.cxx:34-36)
+    f32p = L.Clarity_Convolve.argtypes
+    L2 = C.CDLL(api.LIB_PATH)
+    L2.Clarity_Convolve.argtypes = [C.c_void_p, api.Dim3, C.c_void_p, api.Dim3, C.c_void_p]
+    L2.Clarity_Convolve.restype = C.c_int
+    assert L2.Clarity_Convolve(None, api.Dim3(4, 4, 4), None, api.Dim3(4, 4, 4), None) == 4
+    # non-positive dimensions
+    with pytest.raises(api.ClarityError) as e:
+        api._check(L.Clarity_Convolve(img, api.Dim3(0, 4, 4), img, api.Dim3(4, 4, 4), img))
+    assert e.value.code == api.CLARITY_INVALID_ARGUMENT
+    assert "dimension" in str(e.value)
+    assert f32p is not None
+
+
+@pytest.mark.skipif(gpu_available(), reason="a GPU is present")
+def test_register_without_gpu_is_invalid_operation():
+    code = api.load().Clarity_Register()
+    assert code == api.CLARITY_INVALID_OPERATION
+    img = np.ones((4, 4, 4), np.float32)
+    with pytest.raises(api.ClarityError) as e:
+        api.convolve(img, img)
+    assert e.value.code == api.CLARITY_INVALID_OPERATION
+    assert "Register" in str(e.value)
+
+
+@pytest.mark.parametrize("work", [(16, 32, 32), (64, 128, 128), (128, 512, 512),
+                                  (256, 1024, 1024), (11, 15, 19), (1, 1, 2), (2, 3, 5),
+                                  (176, 608, 544), (32, 192, 640), (96, 448, 224)])
+def test_planner_invariants(work):
+    z, y, x = work
+    p = api.plan_info(work)
+    assert p["Ay"] * p["By"] == y
+    assert p["By"] % p["G"] == 0
+    assert p["KG"] * p["W"] >= p["XS"]
+    assert p["xmode"] == (x % 2)
+    assert p["M"] == (x // 2 if x % 2 == 0 else x)
+    assert p["xy_smem"] <= 200 * 1024 and p["z_smem"] <= 200 * 1024
+    assert p["z_blocks"] == p["Ay"] * p["KG"]
+    assert p["xy_blocks"] == z * (p["By"] // p["G"])
+
+
+def test_planner_rejects_unsupported_prime():
+    with pytest.raises(api.ClarityError) as e:
+        api.plan_info((8, 8, 2 * 23))
+    assert e.value.code == api.CLARITY_INVALID_ARGUMENT

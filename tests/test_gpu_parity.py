@@ -1,0 +1,150 @@
+"""GPU parity: the CUDA library, called through its C ABI, against the
+oracle (the reference's own outputs in tests/golden, and the CPU restatement
+for cases without fixtures).
+
+Tolerances (relative L2 over the output image): 1e-5 for single-pass results
+(Convolve, Wiener, one RL iteration), 1e-4 after several iterations; the error
+against the FP64 oracle is checked to be of the same order as the FP32
+reference's own.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from clarity_b200 import synthetic as syn
+from conftest import load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_ONE = 1e-5
+TOL_ITER = 1e-4
+CASES = ["small_even", "small_odd", "testcommon_16x16x8"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_convolve_golden(clarity_gpu, case):
+    d = load_golden(case)
+    out = clarity_gpu.convolve(d["image"], d["psf"])
+    assert rel_l2(out, d["convolve"]) <= TOL_ONE
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_wiener_golden(clarity_gpu, case):
+    d = load_golden(case)
+    out = clarity_gpu.wiener_deconvolve(d["image"], d["psf"], float(d["wiener_eps"]))
+    assert rel_l2(out, d["wiener"]) <= TOL_ONE
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_rl_one_iteration_golden(clarity_gpu, case):
+    d = load_golden(case)
+    out = clarity_gpu.maximum_likelihood_deconvolve(d["image"], d["psf"], 1)
+    assert rel_l2(out, d["rl1_ref64"]) <= TOL_ONE
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_rl_golden(clarity_gpu, case):
+    d = load_golden(case)
+    out = clarity_gpu.maximum_likelihood_deconvolve(d["image"], d["psf"], int(d["rl_iters"]))
+    assert rel_l2(out, d["rl_ref64"]) <= TOL_ITER
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_jvc_golden(clarity_gpu, case):
+    d = load_golden(case)
+    out = clarity_gpu.jansen_van_cittert_deconvolve(d["image"], d["psf"], int(d["jvc_iters"]))
+    assert rel_l2(out, d["jvc"]) <= TOL_ITER
+    assert out.min() >= 0.0
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_blind_golden(clarity_gpu, case):
+    d = load_golden(case)
+    out = clarity_gpu.blind_maximum_likelihood_deconvolve(d["image"], d["psf"],
+                                                          int(d["blind_iters"]))
+    assert rel_l2(out, d["blind_ref64"]) <= TOL_ITER
+
+
+def test_cfg0_rl10_golden(clarity_gpu, oracle_lib):
+    # 64x64x32 image, same-size PSF, 10 RL iterations
+    d = load_golden("cfg0_rl10")
+    out = clarity_gpu.maximum_likelihood_deconvolve(d["image"], d["psf"], 10)
+    err32 = rel_l2(out, d["rl_ref64"])
+    assert err32 <= TOL_ITER
+    f64 = oracle_lib.rl(d["image"], d["psf"], 10, precision="f64")
+    # the FP32 reference's own distance to FP64 sets the scale
+    ref_err = rel_l2(d["rl_ref64"], f64)
+    assert rel_l2(out, f64) <= max(3 * ref_err, 1e-5)
+
+
+@pytest.mark.parametrize("img_shape,psf_shape", [
+    ((6, 9, 10), (3, 4, 5)),     # work 15x13x9: odd x, primes 13
+    ((5, 8, 12), (3, 3, 5)),     # work 17x11x8: x prime 17 (odd), y 11
+    ((16, 20, 30), (8, 10, 10)), # work 40x30x24
+    ((1, 6, 8), (1, 2, 2)),      # z = 2 work
+    ((3, 1, 9), (2, 1, 3)),      # y = 2 work
+])
+def test_odd_shapes_vs_oracle(clarity_gpu, oracle_lib, img_shape, psf_shape):
+    r = syn.rng(7)
+    img = (r.random(img_shape) * 100 + 1).astype(np.float32)
+    psf = syn.gaussian_psf(psf_shape, 1.0, 1.0).astype(np.float32)
+    assert rel_l2(clarity_gpu.convolve(img, psf), oracle_lib.convolve(img, psf)) <= TOL_ONE
+    assert rel_l2(clarity_gpu.maximum_likelihood_deconvolve(img, psf, 3),
+                  oracle_lib.rl(img, psf, 3)) <= TOL_ITER
+    assert rel_l2(clarity_gpu.wiener_deconvolve(img, psf, 1e-2),
+                  oracle_lib.wiener(img, psf, 1e-2)) <= TOL_ONE
+
+
+def test_cfg1_rl_one_iteration_vs_oracle(clarity_gpu, oracle_lib):
+    # configs[1] size (256x256x64 image, same-size halo PSF): one iteration
+    # against the FP32 restatement (double flux sum)
+    img, psf, _ = syn.cfg1(seed=1)
+    out = clarity_gpu.maximum_likelihood_deconvolve(img, psf, 1)
+    ref = oracle_lib.rl(img, psf, 1)
+    assert rel_l2(out, ref) <= TOL_ONE
+
+
+def test_cfg1_convolve_delta_identity(clarity_gpu):
+    # size-independent property: a centred delta kernel gives the identity
+    img, _, _ = syn.cfg1(seed=2)
+    delta = np.zeros((64, 256, 256), np.float32)
+    delta[32, 128, 128] = 1.0
+    out = clarity_gpu.convolve(img, delta)
+    assert rel_l2(out, img) <= 1e-6
+
+
+def test_iterations_zero_returns_input(clarity_gpu):
+    d = load_golden("small_even")
+    out = clarity_gpu.maximum_likelihood_deconvolve(d["image"], d["psf"], 0)
+    assert np.array_equal(out, d["image"])
+
+
+def test_idivergence_matches_oracle(clarity_gpu, oracle_lib):
+    d = load_golden("small_even")
+    ghat = clarity_gpu.convolve(d["rl_ref64"], d["psf"])
+    a = clarity_gpu.idivergence(d["image"], ghat)
+    b = oracle_lib.idivergence(d["image"], ghat)
+    assert abs(a - b) <= 1e-9 * max(1.0, abs(b))
+
+
+def test_device_alloc_failure_is_reported_and_recovers(clarity_gpu):
+    d = load_golden("small_odd")
+    clarity_gpu.trim()
+    clarity_gpu.inject_device_alloc_failure(1)
+    with pytest.raises(clarity_gpu.ClarityError) as e:
+        clarity_gpu.convolve(d["image"], d["psf"])
+    assert e.value.code == clarity_gpu.CLARITY_DEVICE_OUT_OF_MEMORY
+    out = clarity_gpu.convolve(d["image"], d["psf"])
+    assert rel_l2(out, d["convolve"]) <= TOL_ONE
+
+
+def test_device_api_matches_host_api(clarity_gpu):
+    import torch
+    d = load_golden("small_even")
+    img = torch.from_numpy(d["image"]).cuda()
+    psf = torch.from_numpy(d["psf"]).cuda()
+    out = torch.empty_like(img)
+    clarity_gpu.ml_device(img, psf, out, 5)
+    torch.cuda.synchronize()
+    host = clarity_gpu.maximum_likelihood_deconvolve(d["image"], d["psf"], 5)
+    assert np.array_equal(out.cpu().numpy(), host)
