@@ -12,7 +12,7 @@
 // the smallest prime factor); odd primes use the direct symmetric form that
 // pairs t with N - t (about N^2 real multiply-adds).
 #pragma once
-#include <cuda_runtime.h>
+#include "launch_macro.cuh"
 
 #include <type_traits>
 #include <utility>

@@ -108,159 +108,7 @@ void timing_collect(double* ms, long long* counts) {
   g_events.clear();
 }
 
-// ----------------------------------------------------------------- planner
-static void search_axis(int n, int depth, int* cur, int* best, int* best_len,
-                        int* best_max) {
-  if (n == 1) {
-    int mx = 0;
-    for (int i = 0; i < depth; ++i) mx = std::max(mx, cur[i]);
-    if (depth < *best_len || (depth == *best_len && mx < *best_max)) {
-      *best_len = depth;
-      *best_max = mx;
-      for (int i = 0; i < depth; ++i) best[i] = cur[i];
-    }
-    return;
-  }
-  if (depth >= kMaxPasses || depth + 1 > *best_len) return;
-  for (int r : kRadixSet) {
-    if (n % r == 0) {
-      // keep radices non-increasing to avoid permutations of one factor set
-      if (depth > 0 && r > cur[depth - 1]) continue;
-      cur[depth] = r;
-      search_axis(n / r, depth + 1, cur, best, best_len, best_max);
-    }
-  }
-}
-
-static bool plan_axis(int n, AxisPlan* A) {
-  std::memset(A, 0, sizeof(*A));
-  A->n = n;
-  if (n == 1) return true;
-  int cur[kMaxPasses], best[kMaxPasses];
-  int best_len = kMaxPasses + 1, best_max = INT_MAX;
-  search_axis(n, 0, cur, best, &best_len, &best_max);
-  if (best_len > kMaxPasses) return false;
-  A->npass = best_len;
-  int len = n;
-  for (int s = 0; s < best_len; ++s) {
-    A->radix[s] = best[s];
-    A->len[s] = len;
-    A->span[s] = len / best[s];
-    len /= best[s];
-  }
-  return true;
-}
-
-static int ctz(int v) {
-  int c = 0;
-  while (v && !(v & 1)) { v >>= 1; ++c; }
-  return c;
-}
-
-static constexpr int kSmemMax = 200 * 1024;
-static constexpr int kSmemPerSM = 228 * 1024;
-
-bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
-  VolPlan P;
-  std::memset(&P, 0, sizeof(P));
-  P.nx = nx; P.ny = ny; P.nz = nz;
-  P.xmode = (nx % 2 == 0) ? 0 : 1;
-  P.M = P.xmode == 0 ? nx / 2 : nx;
-  P.XS = P.xmode == 0 ? P.M + 1 : nx;
-  if (P.xmode == 0)
-    P.items = (P.M % 2 == 0) ? std::max(P.M / 2, 1) : (P.M + 1) / 2;
-  else
-    P.items = nx;
-  if (!plan_axis(P.M, &P.ax)) {
-    if (why) *why = "x length " + std::to_string(nx) + " has an unsupported factor";
-    return false;
-  }
-  if (!plan_axis(nz, &P.az)) {
-    if (why) *why = "z length " + std::to_string(nz) + " has an unsupported factor";
-    return false;
-  }
-  // x row padding in the XY shared memory
-  if (P.ax.npass <= 1 || (P.ax.span[0] & 1)) P.padShift = 30;
-  else P.padShift = ctz(P.ax.span[0]);
-  {
-    const int last = P.M - 1;
-    int rs = last + (last >> P.padShift) + 1;
-    if (rs % 2 == 0) rs += 1;
-    P.rowStride = rs;
-  }
-  double best_score = -1e300;
-  VolPlan best = P;
-  bool found = false;
-  std::vector<int> ays = {1};
-  for (int r : kRadixSet) ays.push_back(r);
-  for (int ay : ays) {
-    if (ny % ay) continue;
-    const int by = ny / ay;
-    AxisPlan ab;
-    if (!plan_axis(by, &ab)) continue;
-    for (int W : {1, 2, 4, 8}) {
-      const long long zsm = (long long)nz * by * W * 8;
-      if (zsm > kSmemMax) continue;
-      for (int G = 1; G <= 16; ++G) {
-        if (by % G) continue;
-        const long long xysm = (long long)G * ay * P.rowStride * 8;
-        if (xysm > kSmemMax) continue;
-        const int KG = (P.XS + W - 1) / W;
-        const long long xy_blocks = (long long)nz * (by / G);
-        const long long z_blocks = (long long)ay * KG;
-        const int occ_xy = std::min(8, (int)(kSmemPerSM / (xysm + 1024)));
-        const int occ_z = std::min(8, (int)(kSmemPerSM / (zsm + 1024)));
-        const double seg = (double)G * W * 8;
-        double score = 0;
-        score += 10.0 * std::min(std::min(occ_xy, occ_z), 3);
-        score += seg >= 32 ? 6.0 : seg / 32.0 * 6.0;
-        score += (xy_blocks >= 296 ? 3.0 : 3.0 * xy_blocks / 296.0);
-        score += (z_blocks >= 296 ? 3.0 : 3.0 * z_blocks / 296.0);
-        score -= 4.0 * ((double)KG * W / P.XS - 1.0);
-        score -= 0.05 * std::abs(ay - 16);
-        score -= 0.02 * G;  // prefer fewer rows per tile at equal merit
-        if (score > best_score) {
-          best_score = score;
-          best = P;
-          best.Ay = ay; best.By = by; best.G = G; best.W = W; best.KG = KG;
-          best.ayB = ab;
-          best.xy_smem = (int)xysm;
-          best.z_smem = (int)zsm;
-          best.xy_blocks = (int)xy_blocks;
-          best.z_blocks = (int)z_blocks;
-          found = true;
-        }
-      }
-    }
-  }
-  if (!found) {
-    if (why) *why = "no tiling of y=" + std::to_string(ny) + ", z=" + std::to_string(nz) +
-                    " fits in shared memory with the supported radices";
-    return false;
-  }
-  P = best;
-  P.xy_threads = 256;
-  P.z_threads = 256;
-  P.spec_elems = (long long)P.Ay * P.KG * P.nz * P.By * P.W;
-  // twiddle buffer layout
-  int off = 0;
-  P.ax.tw_off = off; off += std::max(P.M, 1);
-  P.ayB.tw_off = off; off += std::max(P.By, 1);
-  P.az.tw_off = off; off += std::max(P.nz, 1);
-  P.tw_r2c_off = off; off += P.M / 2 + 1;
-  P.tw_ny_off = off; off += P.ny;
-  P.twiddle_count = off;
-  P.xrev_off = 0;
-  P.xrev_count = P.M;
-  *out = P;
-  return true;
-}
-
 // ------------------------------------------------------------ small kernels
-struct TwTable {
-  int off, n, count;
-};
-
 // w_n^t = exp(-2 pi i t / n), evaluated in FP64 with sincospi and rounded.
 __global__ void k_gen_twiddles(float2* tw, const TwTable* tabs, int ntab) {
   for (int k = 0; k < ntab; ++k) {
@@ -441,25 +289,9 @@ Status Context::plan(const Dims& wd, const PlanEntry** out) {
   const VolPlan& P = pe->P;
   CL_CHECK(dev_alloc((void**)&pe->tw, sizeof(float2) * P.twiddle_count));
   CL_CHECK(dev_alloc((void**)&pe->xrev, sizeof(int) * std::max(P.xrev_count, 1)));
-  // digit-reversed slot of each natural x frequency after the DIF passes
-  std::vector<int> rev(std::max(P.M, 1));
-  for (int k = 0; k < P.M; ++k) {
-    int rem = k, pos = 0;
-    for (int s = 0; s < P.ax.npass; ++s) {
-      const int d = rem % P.ax.radix[s];
-      rem /= P.ax.radix[s];
-      pos += d * P.ax.span[s];
-    }
-    rev[k] = pos;
-  }
-  if (P.M == 1) rev[0] = 0;
-  std::vector<TwTable> tabs = {
-      {P.ax.tw_off, std::max(P.M, 1), std::max(P.M, 1)},
-      {P.ayB.tw_off, std::max(P.By, 1), std::max(P.By, 1)},
-      {P.az.tw_off, std::max(P.nz, 1), std::max(P.nz, 1)},
-      {P.tw_r2c_off, P.nx, P.M / 2 + 1},
-      {P.tw_ny_off, P.ny, P.ny},
-  };
+  std::vector<int> rev;
+  std::vector<TwTable> tabs;
+  plan_tables(P, &rev, &tabs);
   TwTable* dtabs = nullptr;
   CL_CHECK(dev_alloc((void**)&dtabs, sizeof(TwTable) * tabs.size()));
   cudaStream_t st = exec_stream();
@@ -467,7 +299,7 @@ Status Context::plan(const Dims& wd, const PlanEntry** out) {
                            cudaMemcpyHostToDevice, st));
   CL_CHECK(cudaMemcpyAsync(dtabs, tabs.data(), sizeof(TwTable) * tabs.size(),
                            cudaMemcpyHostToDevice, st));
-  k_gen_twiddles<<<64, 256, 0, st>>>(pe->tw, dtabs, (int)tabs.size());
+  CLARITY_LAUNCH(k_gen_twiddles, 64, 256, 0, st)(pe->tw, dtabs, (int)tabs.size());
   CL_CHECK(cudaGetLastError());
   CL_CHECK(cudaStreamSynchronize(st));
   cudaFree(dtabs);
@@ -574,9 +406,9 @@ static Status reduce_sum_into(Context& ctx, const float* a, long long n,
                               double* partial, double* dout) {
   cudaStream_t st = ctx.exec_stream();
   count_small();
-  k_reduce_sum<<<kReduceBlocks, 256, 0, st>>>(a, n, partial);
+  CLARITY_LAUNCH(k_reduce_sum, kReduceBlocks, 256, 0, st)(a, n, partial);
   count_small();
-  k_finish_sum<<<1, 256, 0, st>>>(partial, kReduceBlocks, dout);
+  CLARITY_LAUNCH(k_finish_sum, 1, 256, 0, st)(partial, kReduceBlocks, dout);
   CL_CHECK(cudaGetLastError());
   return Status::Ok();
 }
@@ -653,7 +485,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     CL_TRY(xy_inverse(ctx, pe, epi, ws.S));
     if (rescale) {
       count_small();
-      k_finish_rl_scale<<<1, 256, 0, st>>>(ws.partial, P.xy_blocks, ws.dscal + 0,
+      CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws.partial, P.xy_blocks, ws.dscal + 0,
                                            ws.dscal + 1, sdev);
       CL_CHECK(cudaGetLastError());
     }
@@ -671,14 +503,14 @@ Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
   if (iters <= 0) {
     // the reference leaves the output unwritten; return the input image
     count_small();
-    k_copy<<<kReduceBlocks, 256, 0, st>>>(img, out, id.n());
+    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, st)(img, out, id.n());
     CL_CHECK(cudaGetLastError());
     return Status::Ok();
   }
   CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
   CL_TRY(rl_core(ctx, *pe, *ws, img, id, wd, iters, true));
   count_small();
-  k_clip<<<kReduceBlocks, 256, 0, st>>>(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
+  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
                                         ws->fscal);
   CL_CHECK(cudaGetLastError());
   return Status::Ok();
@@ -693,20 +525,20 @@ Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
   cudaStream_t st = ctx.exec_stream();
   if (iters <= 0) {
     count_small();
-    k_copy<<<kReduceBlocks, 256, 0, st>>>(img, out, id.n());
+    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, st)(img, out, id.n());
     CL_CHECK(cudaGetLastError());
     return Status::Ok();
   }
   // h <- h / sum(h) (src/BlindMaximumLikelihoodDeconvolve.cxx:59)
   count_small();
-  k_reduce_sum<<<kReduceBlocks, 256, 0, st>>>(ker, kd.n(), ws->partial);
+  CLARITY_LAUNCH(k_reduce_sum, kReduceBlocks, 256, 0, st)(ker, kd.n(), ws->partial);
   count_small();
-  k_finish_inverse<<<1, 256, 0, st>>>(ws->partial, kReduceBlocks, ws->fscal + 2);
+  CLARITY_LAUNCH(k_finish_inverse, 1, 256, 0, st)(ws->partial, kReduceBlocks, ws->fscal + 2);
   CL_CHECK(cudaGetLastError());
   CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, ws->fscal + 2));
   CL_TRY(rl_core(ctx, *pe, *ws, img, id, wd, iters, false));
   count_small();
-  k_clip<<<kReduceBlocks, 256, 0, st>>>(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
+  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
                                         nullptr);
   CL_CHECK(cudaGetLastError());
   return Status::Ok();
@@ -727,9 +559,9 @@ Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
   // A = max(unpadded image) / 2 (src/JansenVanCittertDeconvolve.cxx:324)
   float* pmax = reinterpret_cast<float*>(ws->partial);
   count_small();
-  k_reduce_max<<<kReduceBlocks, 256, 0, st>>>(img, id.n(), pmax);
+  CLARITY_LAUNCH(k_reduce_max, kReduceBlocks, 256, 0, st)(img, id.n(), pmax);
   count_small();
-  k_finish_jvc<<<1, 32, 0, st>>>(pmax, kReduceBlocks, ws->fscal + 4);
+  CLARITY_LAUNCH(k_finish_jvc, 1, 32, 0, st)(pmax, kReduceBlocks, ws->fscal + 4);
   CL_CHECK(cudaGetLastError());
   // A and invASq are needed as kernel arguments: read them back once.
   float hc[2];
@@ -750,7 +582,7 @@ Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
       CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
   }
   count_small();
-  k_clip<<<kReduceBlocks, 256, 0, st>>>(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
+  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
                                         nullptr);
   CL_CHECK(cudaGetLastError());
   return Status::Ok();
@@ -764,9 +596,9 @@ Status run_idivergence(Context& ctx, const float* g, const float* ghat,
   CL_CHECK(dev_alloc((void**)&part, sizeof(double) * kReduceBlocks));
   CL_CHECK(dev_alloc((void**)&d, sizeof(double)));
   count_small();
-  k_idiv<<<kReduceBlocks, 256, 0, st>>>(g, ghat, n, part);
+  CLARITY_LAUNCH(k_idiv, kReduceBlocks, 256, 0, st)(g, ghat, n, part);
   count_small();
-  k_finish_sum<<<1, 256, 0, st>>>(part, kReduceBlocks, d);
+  CLARITY_LAUNCH(k_finish_sum, 1, 256, 0, st)(part, kReduceBlocks, d);
   cudaError_t e = cudaMemcpyAsync(result, d, sizeof(double), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   cudaFree(part);

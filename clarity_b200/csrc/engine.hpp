@@ -39,8 +39,6 @@ struct PlanEntry {
   int* xrev = nullptr;   // natural x frequency -> smem slot after x passes
 };
 
-// Planner (host only).  Returns false for shapes it cannot decompose.
-bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why);
 
 // Device allocation that honours the host-side fault injector.
 cudaError_t dev_alloc(void** p, size_t bytes);

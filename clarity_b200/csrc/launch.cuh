@@ -21,8 +21,8 @@ template <class K>
 static cudaError_t prep_kernel(K kernel, int smem) {
   // Opt in to the dynamic shared memory this launch needs (idempotent).
   if (smem > 48 * 1024)
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem);
+    return cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   return cudaSuccess;
 }
 
@@ -33,7 +33,7 @@ Status xy_forward(Context& ctx, const PlanEntry& pe, const Pro& pro,
   auto k = k_xy_forward<Pro>;
   CL_CHECK(prep_kernel(k, P.xy_smem));
   note_launch_begin(KK_XY_FORWARD, ctx.exec_stream());
-  k<<<P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream()>>>(P, pro, S, pe.tw,
+  CLARITY_LAUNCH(k, P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream())(P, pro, S, pe.tw,
                                                                  pe.xrev);
   note_launch_end(KK_XY_FORWARD, ctx.exec_stream());
   CL_CHECK(cudaGetLastError());
@@ -47,7 +47,7 @@ Status xy_inverse(Context& ctx, const PlanEntry& pe, const Epi& epi,
   auto k = k_xy_inverse<Epi>;
   CL_CHECK(prep_kernel(k, P.xy_smem));
   note_launch_begin(KK_XY_INVERSE, ctx.exec_stream());
-  k<<<P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream()>>>(P, epi, S, pe.tw,
+  CLARITY_LAUNCH(k, P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream())(P, epi, S, pe.tw,
                                                                  pe.xrev);
   note_launch_end(KK_XY_INVERSE, ctx.exec_stream());
   CL_CHECK(cudaGetLastError());
@@ -61,7 +61,7 @@ Status xy_inv_fwd(Context& ctx, const PlanEntry& pe, const Mid& mid,
   auto k = k_xy_inv_fwd<Mid>;
   CL_CHECK(prep_kernel(k, P.xy_smem));
   note_launch_begin(KK_XY_INV_FWD, ctx.exec_stream());
-  k<<<P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream()>>>(P, mid, S, pe.tw,
+  CLARITY_LAUNCH(k, P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream())(P, mid, S, pe.tw,
                                                                  pe.xrev);
   note_launch_end(KK_XY_INV_FWD, ctx.exec_stream());
   CL_CHECK(cudaGetLastError());
@@ -75,7 +75,7 @@ Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
   auto k = k_z<Mod>;
   CL_CHECK(prep_kernel(k, P.z_smem));
   note_launch_begin(KK_Z, ctx.exec_stream());
-  k<<<P.z_blocks, P.z_threads, P.z_smem, ctx.exec_stream()>>>(P, mod, Sin, Sout,
+  CLARITY_LAUNCH(k, P.z_blocks, P.z_threads, P.z_smem, ctx.exec_stream())(P, mod, Sin, Sout,
                                                               pe.tw);
   note_launch_end(KK_Z, ctx.exec_stream());
   CL_CHECK(cudaGetLastError());

@@ -8,7 +8,7 @@
 // Spectral operations (Z pass): apply(idx, v) with idx the element's offset
 //   in the S layout (the OTF shares that layout).
 #pragma once
-#include <cuda_runtime.h>
+#include "launch_macro.cuh"
 
 #include "dft_codelets.cuh"
 #include "plan.hpp"

@@ -7,7 +7,7 @@
 // src/ComputePrimitivesGPU.cu:148-239 and src/JansenVanCittertDeconvolveGPU.cu
 // :38-75, which here become prologues and epilogues of the FFT passes.
 #pragma once
-#include <cuda_runtime.h>
+#include "launch_macro.cuh"
 
 #include "dft_codelets.cuh"
 #include "plan.hpp"
@@ -482,7 +482,7 @@ template <class Pro>
 __global__ void __launch_bounds__(256, 2)
     k_xy_forward(const VolPlan P, const Pro pro, float2* __restrict__ S,
                  const float2* __restrict__ tw, const int* __restrict__ xrev) {
-  extern __shared__ float2 sm[];
+  CLARITY_DYN_SMEM(float2, sm);
   const int ngroups = P.By / P.G;
   const int z = blockIdx.x / ngroups;
   const int y0base = (blockIdx.x - z * ngroups) * P.G;
@@ -498,7 +498,7 @@ template <class Epi>
 __global__ void __launch_bounds__(256, 2)
     k_xy_inverse(const VolPlan P, Epi epi, const float2* __restrict__ S,
                  const float2* __restrict__ tw, const int* __restrict__ xrev) {
-  extern __shared__ float2 sm[];
+  CLARITY_DYN_SMEM(float2, sm);
   const int ngroups = P.By / P.G;
   const int z = blockIdx.x / ngroups;
   const int y0base = (blockIdx.x - z * ngroups) * P.G;
@@ -516,7 +516,7 @@ template <class Mid>
 __global__ void __launch_bounds__(256, 2)
     k_xy_inv_fwd(const VolPlan P, Mid mid, float2* __restrict__ S,
                  const float2* __restrict__ tw, const int* __restrict__ xrev) {
-  extern __shared__ float2 sm[];
+  CLARITY_DYN_SMEM(float2, sm);
   const int ngroups = P.By / P.G;
   const int z = blockIdx.x / ngroups;
   const int y0base = (blockIdx.x - z * ngroups) * P.G;
@@ -539,7 +539,7 @@ template <class Mod>
 __global__ void __launch_bounds__(256, 2)
     k_z(const VolPlan P, const Mod mod, const float2* __restrict__ Sin,
         float2* __restrict__ Sout, const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
+  CLARITY_DYN_SMEM(float2, sm);
   const long long tile = (long long)P.nz * P.By * P.W;
   const long long base = (long long)blockIdx.x * tile;
   // load (16-byte vectors when the tile size is even, which keeps every

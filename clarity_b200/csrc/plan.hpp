@@ -23,6 +23,8 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <string>
+#include <vector>
 
 namespace clarity {
 
@@ -66,6 +68,17 @@ struct VolPlan {
   int xy_smem, z_smem;   // bytes of dynamic shared memory
   long long n_real() const { return (long long)nx * ny * nz; }
 };
+
+// Twiddle table w_n^t = exp(-2 pi i t / n), t < count, at float2 offset off.
+struct TwTable {
+  int off, n, count;
+};
+// The digit-reversed slot of each natural x frequency after the x DIF
+// passes, and the twiddle tables a plan needs.
+void plan_tables(const VolPlan& P, std::vector<int>* xrev, std::vector<TwTable>* tabs);
+
+// Planner (host only).  Returns false for shapes it cannot decompose.
+bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why);
 
 // Radices accepted for one register pass (must match dft_codelets.cuh).
 constexpr int kRadixSet[] = {16, 19, 17, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};

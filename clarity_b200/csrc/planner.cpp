@@ -1,0 +1,181 @@
+// planner.cpp -- host-only planning of the fused FFT passes for one work
+// box (see plan.hpp for the pass structure and the S layout).
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace clarity {
+
+static void search_axis(int n, int depth, int* cur, int* best, int* best_len,
+                        int* best_max) {
+  if (n == 1) {
+    int mx = 0;
+    for (int i = 0; i < depth; ++i) mx = std::max(mx, cur[i]);
+    if (depth < *best_len || (depth == *best_len && mx < *best_max)) {
+      *best_len = depth;
+      *best_max = mx;
+      for (int i = 0; i < depth; ++i) best[i] = cur[i];
+    }
+    return;
+  }
+  if (depth >= kMaxPasses || depth + 1 > *best_len) return;
+  for (int r : kRadixSet) {
+    if (n % r == 0) {
+      // keep radices non-increasing to avoid permutations of one factor set
+      if (depth > 0 && r > cur[depth - 1]) continue;
+      cur[depth] = r;
+      search_axis(n / r, depth + 1, cur, best, best_len, best_max);
+    }
+  }
+}
+
+static bool plan_axis(int n, AxisPlan* A) {
+  std::memset(A, 0, sizeof(*A));
+  A->n = n;
+  if (n == 1) return true;
+  int cur[kMaxPasses], best[kMaxPasses];
+  int best_len = kMaxPasses + 1, best_max = INT_MAX;
+  search_axis(n, 0, cur, best, &best_len, &best_max);
+  if (best_len > kMaxPasses) return false;
+  A->npass = best_len;
+  int len = n;
+  for (int s = 0; s < best_len; ++s) {
+    A->radix[s] = best[s];
+    A->len[s] = len;
+    A->span[s] = len / best[s];
+    len /= best[s];
+  }
+  return true;
+}
+
+static int ctz(int v) {
+  int c = 0;
+  while (v && !(v & 1)) { v >>= 1; ++c; }
+  return c;
+}
+
+static constexpr int kSmemMax = 200 * 1024;
+static constexpr int kSmemPerSM = 228 * 1024;
+
+bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
+  VolPlan P;
+  std::memset(&P, 0, sizeof(P));
+  P.nx = nx; P.ny = ny; P.nz = nz;
+  P.xmode = (nx % 2 == 0) ? 0 : 1;
+  P.M = P.xmode == 0 ? nx / 2 : nx;
+  P.XS = P.xmode == 0 ? P.M + 1 : nx;
+  if (P.xmode == 0)
+    P.items = (P.M % 2 == 0) ? std::max(P.M / 2, 1) : (P.M + 1) / 2;
+  else
+    P.items = nx;
+  if (!plan_axis(P.M, &P.ax)) {
+    if (why) *why = "x length " + std::to_string(nx) + " has an unsupported factor";
+    return false;
+  }
+  if (!plan_axis(nz, &P.az)) {
+    if (why) *why = "z length " + std::to_string(nz) + " has an unsupported factor";
+    return false;
+  }
+  // x row padding in the XY shared memory
+  if (P.ax.npass <= 1 || (P.ax.span[0] & 1)) P.padShift = 30;
+  else P.padShift = ctz(P.ax.span[0]);
+  {
+    const int last = P.M - 1;
+    int rs = last + (last >> P.padShift) + 1;
+    if (rs % 2 == 0) rs += 1;
+    P.rowStride = rs;
+  }
+  double best_score = -1e300;
+  VolPlan best = P;
+  bool found = false;
+  std::vector<int> ays = {1};
+  for (int r : kRadixSet) ays.push_back(r);
+  for (int ay : ays) {
+    if (ny % ay) continue;
+    const int by = ny / ay;
+    AxisPlan ab;
+    if (!plan_axis(by, &ab)) continue;
+    for (int W : {1, 2, 4, 8}) {
+      const long long zsm = (long long)nz * by * W * 8;
+      if (zsm > kSmemMax) continue;
+      for (int G = 1; G <= 16; ++G) {
+        if (by % G) continue;
+        const long long xysm = (long long)G * ay * P.rowStride * 8;
+        if (xysm > kSmemMax) continue;
+        const int KG = (P.XS + W - 1) / W;
+        const long long xy_blocks = (long long)nz * (by / G);
+        const long long z_blocks = (long long)ay * KG;
+        const int occ_xy = std::min(8, (int)(kSmemPerSM / (xysm + 1024)));
+        const int occ_z = std::min(8, (int)(kSmemPerSM / (zsm + 1024)));
+        const double seg = (double)G * W * 8;
+        double score = 0;
+        score += 10.0 * std::min(std::min(occ_xy, occ_z), 3);
+        score += seg >= 32 ? 6.0 : seg / 32.0 * 6.0;
+        score += (xy_blocks >= 296 ? 3.0 : 3.0 * xy_blocks / 296.0);
+        score += (z_blocks >= 296 ? 3.0 : 3.0 * z_blocks / 296.0);
+        score -= 4.0 * ((double)KG * W / P.XS - 1.0);
+        score -= 0.05 * std::abs(ay - 16);
+        score -= 0.02 * G;  // prefer fewer rows per tile at equal merit
+        if (score > best_score) {
+          best_score = score;
+          best = P;
+          best.Ay = ay; best.By = by; best.G = G; best.W = W; best.KG = KG;
+          best.ayB = ab;
+          best.xy_smem = (int)xysm;
+          best.z_smem = (int)zsm;
+          best.xy_blocks = (int)xy_blocks;
+          best.z_blocks = (int)z_blocks;
+          found = true;
+        }
+      }
+    }
+  }
+  if (!found) {
+    if (why) *why = "no tiling of y=" + std::to_string(ny) + ", z=" + std::to_string(nz) +
+                    " fits in shared memory with the supported radices";
+    return false;
+  }
+  P = best;
+  P.xy_threads = 256;
+  P.z_threads = 256;
+  P.spec_elems = (long long)P.Ay * P.KG * P.nz * P.By * P.W;
+  // twiddle buffer layout
+  int off = 0;
+  P.ax.tw_off = off; off += std::max(P.M, 1);
+  P.ayB.tw_off = off; off += std::max(P.By, 1);
+  P.az.tw_off = off; off += std::max(P.nz, 1);
+  P.tw_r2c_off = off; off += P.M / 2 + 1;
+  P.tw_ny_off = off; off += P.ny;
+  P.twiddle_count = off;
+  P.xrev_off = 0;
+  P.xrev_count = P.M;
+  *out = P;
+  return true;
+}
+
+
+void plan_tables(const VolPlan& P, std::vector<int>* xrev, std::vector<TwTable>* tabs) {
+  xrev->assign(std::max(P.M, 1), 0);
+  for (int k = 0; k < P.M; ++k) {
+    int rem = k, pos = 0;
+    for (int s = 0; s < P.ax.npass; ++s) {
+      const int d = rem % P.ax.radix[s];
+      rem /= P.ax.radix[s];
+      pos += d * P.ax.span[s];
+    }
+    (*xrev)[k] = pos;
+  }
+  *tabs = {
+      {P.ax.tw_off, std::max(P.M, 1), std::max(P.M, 1)},
+      {P.ayB.tw_off, std::max(P.By, 1), std::max(P.By, 1)},
+      {P.az.tw_off, std::max(P.nz, 1), std::max(P.nz, 1)},
+      {P.tw_r2c_off, P.nx, P.M / 2 + 1},
+      {P.tw_ny_off, P.ny, P.ny},
+  };
+}
+
+}  // namespace clarity

@@ -1,0 +1,78 @@
+// emu_cuda.hpp -- TEST INFRASTRUCTURE: host emulation of the few CUDA device
+// facilities the library's kernels use, so the kernel sources compile as
+// plain C++ (g++, CLARITY_HOST_EMULATION) and run on the CPU under
+// AddressSanitizer.  Each block runs on one host thread with blockDim.x == 1:
+// every phase's strided loop then covers all its work items and
+// __syncthreads is a no-op, which preserves the kernels' semantics.
+// Dynamic shared memory is a fresh heap buffer per block, filled with NaN
+// bytes so reads of unwritten shared memory poison the result.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+namespace clarity_emu {
+extern thread_local uint3 tIdx, bIdx;
+extern thread_local dim3 bDim, gDim;
+extern thread_local void* smem_ptr;
+
+template <class T>
+T* dynamic_smem() {
+  return static_cast<T*>(smem_ptr);
+}
+
+struct Launcher {
+  long long grid;
+  size_t smem;
+  template <class K>
+  auto operator()(K kernel) const {
+    const long long g = grid;
+    const size_t s = smem;
+    return [g, s, kernel](auto... args) {
+      for (long long b = 0; b < g; ++b) {
+        bIdx = make_uint3((unsigned)b, 0, 0);
+        tIdx = make_uint3(0, 0, 0);
+        bDim = dim3(1, 1, 1);
+        gDim = dim3((unsigned)g, 1, 1);
+        void* p = nullptr;
+        if (s) {
+          p = std::malloc(s);
+          std::memset(p, 0xff, s);
+        }
+        smem_ptr = p;
+        kernel(args...);
+        std::free(p);
+        smem_ptr = nullptr;
+      }
+    };
+  }
+};
+inline Launcher launcher(long long grid, size_t smem) { return Launcher{grid, smem}; }
+}  // namespace clarity_emu
+
+#ifndef __noinline__
+#define __noinline__
+#endif
+#ifndef __launch_bounds__
+#define __launch_bounds__(...)
+#endif
+
+#define threadIdx ::clarity_emu::tIdx
+#define blockIdx ::clarity_emu::bIdx
+#define blockDim ::clarity_emu::bDim
+#define gridDim ::clarity_emu::gDim
+
+template <class T>
+inline T __ldg(const T* p) {
+  return *p;
+}
+// A single lane per warp: partners contribute nothing to a sum.
+inline float __shfl_xor_sync(unsigned, float, int) { return 0.f; }
+inline double __shfl_xor_sync(unsigned, double, int) { return 0.0; }
+inline void __syncthreads() {}
+inline void sincospi(double x, double* s, double* c) {
+  *s = std::sin(M_PI * x);
+  *c = std::cos(M_PI * x);
+}
