@@ -53,6 +53,7 @@ EXTENSION_SYMBOLS = [
     "clarityx_wiener_device", "clarityx_ml_device", "clarityx_blind_ml_device",
     "clarityx_jvc_device", "clarityx_idivergence", "clarityx_plan_info",
     "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
+    "clarityx_convolve_noalloc",
 ]
 
 
@@ -132,6 +133,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_idivergence.restype = i
         L.clarityx_plan_info.argtypes = [Dim3, C.POINTER(C.c_int), i]
         L.clarityx_plan_info.restype = i
+        L.clarityx_convolve_noalloc.argtypes = [vp, Dim3, vp, Dim3, vp, vp]
+        L.clarityx_convolve_noalloc.restype = i
         L.clarityx_launch_count.restype = C.c_longlong
         L.clarityx_timing_enable.argtypes = [i]
         L.clarityx_timing_enable.restype = None
@@ -322,6 +325,12 @@ def _dev(name, image, kernel, out, extra, stream):
 
 def convolve_device(image, kernel, out, stream=None):
     return _dev("clarityx_convolve_device", image, kernel, out, [], stream)
+
+
+def convolve_noalloc(image, kernel, out, stream=None):
+    """clarityx_convolve_noalloc: convolution of device tensors with all
+    scratch in the library's fixed 32 MiB device array (no allocation)."""
+    return _dev("clarityx_convolve_noalloc", image, kernel, out, [], stream)
 
 
 def wiener_device(image, kernel, out, epsilon, stream=None):

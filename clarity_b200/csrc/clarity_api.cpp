@@ -30,7 +30,7 @@ int g_refcount = 0;              // src/Clarity.cxx:41 (made thread-safe)
 int g_device = 0;
 Context* g_ctx = nullptr;
 unsigned g_threads = 0;
-thread_local std::string g_last_error;
+thread_local char g_last_error[512];
 
 // Staging buffers for the host-buffer API (grown on demand).
 struct Staging {
@@ -40,14 +40,18 @@ struct Staging {
   size_t img_cap = 0, ker_cap = 0, out_cap = 0;
 } g_stage;
 
+void set_error(const char* msg) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg ? msg : "");
+}
+
 ClarityResult_t fail(ClarityResult_t code, const std::string& msg) {
-  g_last_error = msg;
+  set_error(msg.c_str());
   return code;
 }
 
 ClarityResult_t report(const Status& s) {
   if (s.ok()) return CLARITY_SUCCESS;
-  g_last_error = s.msg;
+  set_error(s.msg.c_str());
   return s.code;
 }
 
@@ -135,6 +139,9 @@ ClarityResult_t device_call(const float* in, Clarity_Dim3 id, const float* ker,
 
 namespace clarity {
 Context* global_context() { return g_ctx; }
+// Records the message returned by clarityx_last_error (fixed buffer, no
+// allocation).
+void set_last_error(const char* msg) { set_error(msg); }
 }  // namespace clarity
 
 // ================================================================== public
@@ -335,7 +342,7 @@ ClarityResult_t Clarity_Convolve(float* inImage, Clarity_Dim3 imageDim, float* k
 
 // ============================================================== extensions
 
-const char* clarityx_last_error(void) { return g_last_error.c_str(); }
+const char* clarityx_last_error(void) { return g_last_error; }
 
 ClarityResult_t clarityx_set_device(int device) {
   std::lock_guard<std::mutex> lk(g_mu);

@@ -102,6 +102,7 @@ Status run_idivergence(Context& ctx, const float* g, const float* ghat,
                        long long n, double* result);
 
 Context* global_context();  // nullptr when not registered
+void set_last_error(const char* msg);
 
 // ------------------------------------------------ launch accounting
 // Kernel families timed by the optional event probes.

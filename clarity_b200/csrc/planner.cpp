@@ -92,9 +92,14 @@ bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
   double best_score = -1e300;
   VolPlan best = P;
   bool found = false;
-  std::vector<int> ays = {1};
-  for (int r : kRadixSet) ays.push_back(r);
-  for (int ay : ays) {
+  // candidate Ay: 1 and every register radix (fixed array: planning
+  // allocates nothing)
+  int ays[1 + sizeof(kRadixSet) / sizeof(kRadixSet[0])];
+  int nays = 0;
+  ays[nays++] = 1;
+  for (int r : kRadixSet) ays[nays++] = r;
+  for (int ai = 0; ai < nays; ++ai) {
+    const int ay = ays[ai];
     if (ny % ay) continue;
     const int by = ny / ay;
     AxisPlan ab;

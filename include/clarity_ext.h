@@ -65,6 +65,28 @@ CLARITY_API ClarityResult_t clarityx_idivergence(const float *g,
 CLARITY_API ClarityResult_t clarityx_plan_info(Clarity_Dim3 workDim,
                                                int *fields, int nfields);
 
+/* Circular convolution of device buffers that allocates nothing (no
+ * cudaMalloc, cudaFree or allocating library call; no Clarity_Register
+ * needed).  It has no counterpart in the reference.  It is for callers that
+ * cannot allocate device memory once running: work recorded into CUDA graphs
+ * or run under the caller's own memory pool, fixed-footprint real-time
+ * loops, and plugins hosted in a context that forbids cudaMalloc.
+ * image/kernel/out are device buffers on the current device, as in
+ * clarityx_convolve_device, and the result is the same.
+ * Scratch: one 32 MiB array in the library's device memory (held by every
+ * GPU that loads the library until exit), enough for a padded work box of
+ * 128 x 128 x 128 voxels; larger boxes return CLARITY_INVALID_ARGUMENT
+ * with the size needed in clarityx_last_error().  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.
+ * Every call shares the one array: calls that overlap on the GPU (two
+ * streams, two host threads) race and corrupt each other's results, so
+ * serialise them.  Nothing in the array needs to start at zero; each call
+ * rewrites what it reads. */
+CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, void *stream);
+
 /* Benchmark probes.  clarityx_launch_count: kernels the library has
  * launched so far.  clarityx_timing_enable(1) makes every fused-pass launch
  * record a CUDA event pair on its stream; clarityx_timing_collect waits for

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/clarity.h"
+#include "../../include/clarity_ext.h"
 
 static std::vector<float> read_raw(const char* path, size_t n) {
   std::vector<float> v(n);
@@ -43,6 +44,8 @@ int main(int argc, char** argv) {
                                                  (int)param);
   else if (op == "jvc")
     r = Clarity_JansenVanCittertDeconvolve(img.data(), id, psf.data(), kd, out.data(), (int)param);
+  else if (op == "convolve_noalloc")  // emulated device memory is host memory
+    r = clarityx_convolve_noalloc(img.data(), id, psf.data(), kd, out.data(), nullptr);
   else if (op == "wiener")
     r = Clarity_WienerDeconvolve(img.data(), id, psf.data(), kd, out.data(), (float)param);
   else

@@ -50,6 +50,14 @@ cudaError_t cudaGetDeviceProperties_v2(cudaDeviceProp* p, int) {
   return cudaSuccess;
 }
 cudaError_t cudaGetLastError(void) { return cudaSuccess; }
+cudaError_t cudaGetDevice(int* d) {
+  *d = 0;
+  return cudaSuccess;
+}
+cudaError_t cudaGetSymbolAddress(void** p, const void* symbol) {
+  *p = const_cast<void*>(symbol);
+  return cudaSuccess;
+}
 const char* cudaGetErrorString(cudaError_t e) {
   return e == cudaSuccess ? "no error" : "emulated error";
 }

@@ -59,6 +59,8 @@ def test_emulated_library_matches_reference_golden(emu, tmp_path, case):
     d = load_golden(case)
     img, psf = d["image"], d["psf"]
     assert rel_l2(run_emu(emu, tmp_path, "convolve", img, psf, 0), d["convolve"]) <= 1e-6
+    assert rel_l2(run_emu(emu, tmp_path, "convolve_noalloc", img, psf, 0),
+                  d["convolve"]) <= 1e-6
     assert rel_l2(run_emu(emu, tmp_path, "wiener", img, psf, float(d["wiener_eps"])),
                   d["wiener"]) <= 2e-6
     assert rel_l2(run_emu(emu, tmp_path, "rl", img, psf, 1), d["rl1_ref64"]) <= 1e-6
