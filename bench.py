@@ -232,6 +232,16 @@ def run_gpu_arm(args, rank, world):
     vox = int(np.prod(IMAGE_ZYX))
     value = world * vox * ITERS / (ms_step / 1e3) / 1e9
 
+    if args.quick:
+        api.unregister()
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"quick": True, "ms_per_step": ms_step, "value": value,
+                              "families": {k: v for k, v in fam.items()}}), flush=True)
+        return
+
     # end to end through the public C API with pinned host buffers
     img_h = torch.empty(IMAGE_ZYX, dtype=torch.float32, pin_memory=True).numpy()
     psf_h = torch.empty(IMAGE_ZYX, dtype=torch.float32, pin_memory=True).numpy()
@@ -325,9 +335,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-iters", type=int, default=4)
+    ap.add_argument("--iters", type=int, default=ITERS,
+                    help="RL iterations per step (200 is the workload; fewer only "
+                         "for profiling captures)")
+    ap.add_argument("--quick", action="store_true",
+                    help="device leg only (no e2e, no CPU baseline): for ncu captures")
     args = ap.parse_args()
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
+    global ITERS
+    ITERS = args.iters
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:
