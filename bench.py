@@ -329,6 +329,7 @@ def run_gpu_arm(args, rank, world):
 
 
 def main():
+    global ITERS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -343,7 +344,6 @@ def main():
     args = ap.parse_args()
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
-    global ITERS
     ITERS = args.iters
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
