@@ -12,6 +12,7 @@
 #include <atomic>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.hpp"
@@ -88,6 +89,14 @@ void note_launch_end(int kind, cudaStream_t st) {
 }
 
 long long launch_count() { return g_launches.load(); }
+
+int static_family_mask() {
+  static const int mask = [] {
+    const char* v = std::getenv("CLARITY_STATIC");
+    return v ? std::atoi(v) : 0xF;
+  }();
+  return mask;
+}
 
 static inline void count_small() { g_launches.fetch_add(1); }
 

@@ -114,6 +114,7 @@ enum KernelKind { KK_XY_FORWARD = 0, KK_Z = 1, KK_XY_INV_FWD = 2, KK_XY_INVERSE 
 void note_launch_begin(int kind, cudaStream_t st);
 void note_launch_end(int kind, cudaStream_t st);
 long long launch_count();
+int static_family_mask();
 void timing_enable(bool on);
 // Synchronises the recorded events and returns per-kind totals (ms) and
 // counts; clears the record.

@@ -9,6 +9,17 @@
 
 namespace clarity {
 
+// Compile-time specialised launches (static_dispatch.cuh, instantiated in
+// kern_static_*.cu).  Each returns true when it launched (error in *err).
+template <class F>
+bool static_xy_forward(const PlanEntry&, cudaStream_t, const F&, float2*, cudaError_t*);
+template <class F>
+bool static_z(const PlanEntry&, cudaStream_t, const F&, const float2*, float2*, cudaError_t*);
+template <class F>
+bool static_xy_inv_fwd(const PlanEntry&, cudaStream_t, const F&, float2*, cudaError_t*);
+template <class F>
+bool static_xy_inverse(const PlanEntry&, cudaStream_t, const F&, const float2*, cudaError_t*);
+
 #ifndef CL_CHECK
 #define CL_CHECK(call)                                         \
   do {                                                         \
@@ -30,6 +41,9 @@ template <class Pro>
 Status xy_forward(Context& ctx, const PlanEntry& pe, const Pro& pro,
                          float2* S) {
   const VolPlan& P = pe.P;
+  cudaError_t se = cudaSuccess;
+  if (static_xy_forward(pe, ctx.exec_stream(), pro, S, &se))
+    return status_from_cuda(se, "xy forward");
   auto k = k_xy_forward<Pro>;
   CL_CHECK(prep_kernel(k, P.xy_smem));
   note_launch_begin(KK_XY_FORWARD, ctx.exec_stream());
@@ -44,6 +58,9 @@ template <class Epi>
 Status xy_inverse(Context& ctx, const PlanEntry& pe, const Epi& epi,
                          const float2* S) {
   const VolPlan& P = pe.P;
+  cudaError_t se = cudaSuccess;
+  if (static_xy_inverse(pe, ctx.exec_stream(), epi, S, &se))
+    return status_from_cuda(se, "xy inverse");
   auto k = k_xy_inverse<Epi>;
   CL_CHECK(prep_kernel(k, P.xy_smem));
   note_launch_begin(KK_XY_INVERSE, ctx.exec_stream());
@@ -58,6 +75,9 @@ template <class Mid>
 Status xy_inv_fwd(Context& ctx, const PlanEntry& pe, const Mid& mid,
                          float2* S) {
   const VolPlan& P = pe.P;
+  cudaError_t se = cudaSuccess;
+  if (static_xy_inv_fwd(pe, ctx.exec_stream(), mid, S, &se))
+    return status_from_cuda(se, "xy inverse+forward");
   auto k = k_xy_inv_fwd<Mid>;
   CL_CHECK(prep_kernel(k, P.xy_smem));
   note_launch_begin(KK_XY_INV_FWD, ctx.exec_stream());
@@ -72,6 +92,9 @@ template <class Mod>
 Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
                      const float2* Sin, float2* Sout) {
   const VolPlan& P = pe.P;
+  cudaError_t se = cudaSuccess;
+  if (static_z(pe, ctx.exec_stream(), mod, Sin, Sout, &se))
+    return status_from_cuda(se, "z pass");
   auto k = k_z<Mod>;
   CL_CHECK(prep_kernel(k, P.z_smem));
   note_launch_begin(KK_Z, ctx.exec_stream());

@@ -10,9 +10,13 @@
 #define CLARITY_LAUNCH(kernel, grid, block, smem, stream) \
   kernel<<<(grid), (block), (smem), (stream)>>>
 #define CLARITY_DYN_SMEM(T, name) extern __shared__ T name[]
+// Loop stride of a block-wide strided loop in kernels launched with a
+// compile-time block size.
+#define CLARITY_BLOCK_STRIDE(n) (n)
 #else
 #include "emu_cuda.hpp"
 #define CLARITY_LAUNCH(kernel, grid, block, smem, stream) \
   ::clarity_emu::launcher((grid), (smem))(kernel)
 #define CLARITY_DYN_SMEM(T, name) T* name = ::clarity_emu::dynamic_smem<T>()
+#define CLARITY_BLOCK_STRIDE(n) ((int)blockDim.x)
 #endif

@@ -1,0 +1,545 @@
+// passes_static.cuh -- the fused FFT pass kernels specialised at compile time
+// for the work-box shapes that matter most (the benchmark and test
+// configurations).  Same data layout, digit orders and twiddle tables as the
+// runtime-generic kernels in passes.cuh (the planner produces identical
+// plans), so the two paths can be mixed freely; here every radix, stride and
+// divisor is a constant, the x digit-reversal is computed instead of looked
+// up, and the spectral operation of the Z pass is fused into its last
+// forward / first inverse register pass.
+#pragma once
+#include "dft_codelets.cuh"
+#include "launch_macro.cuh"
+#include "plan.hpp"
+
+namespace clarity {
+namespace st {
+
+// DIF radix sequence of one axis (1 = pass unused).
+template <int R0, int R1 = 1, int R2 = 1>
+struct Rad {
+  static constexpr int n = R0 * R1 * R2;
+  static constexpr int npass = (R0 > 1) + (R1 > 1) + (R2 > 1);
+  static constexpr int radix(int s) { return s == 0 ? R0 : (s == 1 ? R1 : R2); }
+  static constexpr int len(int s) { return s == 0 ? n : (s == 1 ? n / R0 : n / (R0 * R1)); }
+  static constexpr int span(int s) { return len(s) / radix(s); }
+};
+
+constexpr int ctz_c(int v) {
+  int c = 0;
+  while (v > 1 && !(v & 1)) { v >>= 1; ++c; }
+  return c;
+}
+
+// Even nx only (half-length complex rows).
+template <class XR, int AY_, class YR, class ZR, int G_, int W_>
+struct Shape {
+  using X = XR;
+  using Y = YR;
+  using Z = ZR;
+  static constexpr int M = X::n, AY = AY_, BY = Y::n, NZ = Z::n, G = G_, W = W_;
+  static constexpr int NX = 2 * M, NY = AY * BY;
+  static constexpr int XS = M + 1, KG = (XS + W - 1) / W;
+  static constexpr int PADSHIFT =
+      (X::npass <= 1 || (X::span(0) & 1)) ? 30 : ctz_c(X::span(0));
+  static constexpr int ROWSTRIDE_RAW = (M - 1) + ((M - 1) >> PADSHIFT) + 1;
+  static constexpr int ROWSTRIDE = (ROWSTRIDE_RAW % 2 == 0) ? ROWSTRIDE_RAW + 1 : ROWSTRIDE_RAW;
+  static constexpr int ROWS = G * AY;
+  static constexpr int ITEMS = (M % 2 == 0) ? (M / 2 > 1 ? M / 2 : 1) : (M + 1) / 2;
+  static constexpr int BW = BY * W;
+  static constexpr int TILE = NZ * BW;
+  static constexpr int THREADS = 256;
+  static constexpr int XY_SMEM = ROWS * ROWSTRIDE * 8;
+  static constexpr int Z_SMEM = TILE * 8;
+  static constexpr int NGROUPS = BY / G;
+};
+
+template <class SH>
+__device__ __forceinline__ int xp(int e) {
+  return e + (e >> SH::PADSHIFT);
+}
+
+// Digit-reversed slot of natural x frequency k after the DIF passes.
+template <class SH>
+__device__ __forceinline__ int xrev(int k) {
+  using X = typename SH::X;
+  int pos = 0, rem = k;
+#pragma unroll
+  for (int s = 0; s < X::npass; ++s) {
+    const int d = rem % X::radix(s);
+    rem /= X::radix(s);
+    pos += d * X::span(s);
+  }
+  return pos;
+}
+
+template <class SH>
+__device__ __forceinline__ long long sidx(int k1, int kx, int z, int y0) {
+  const int kg = kx / SH::W, ki = kx % SH::W;
+  return ((((long long)k1 * SH::KG + kg) * SH::NZ + z) * SH::BY + y0) * SH::W + ki;
+}
+
+// ------------------------------------------------------------------ x rows
+// One register pass S of the x axis over all rows of the XY tile.
+template <class SH, int S, int DIR>
+__device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw) {
+  using X = typename SH::X;
+  constexpr int R = X::radix(S), len = X::len(S), span = len / R;
+  constexpr int per_row = X::n / R, total = SH::ROWS * per_row, twstep = X::n / len;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int r = f / per_row;
+    const int rem = f - r * per_row;
+    const int b = rem / span;
+    const int i = rem - b * span;
+    float2* row = sm + r * SH::ROWSTRIDE;
+    const int e0 = b * len + i;
+    float2 v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = row[xp<SH>(e0 + t * span)];
+    if constexpr (DIR < 0) {
+      dft<R, -1>(v);
+      if (span > 1 && i != 0) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k * twstep]));
+      }
+    } else {
+      if (span > 1 && i != 0) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k * twstep]));
+      }
+      dft<R, +1>(v);
+    }
+#pragma unroll
+    for (int t = 0; t < R; ++t) row[xp<SH>(e0 + t * span)] = v[t];
+  }
+}
+
+template <class SH, int S>
+__device__ __forceinline__ void x_forward_from(float2* sm, const float2* tw) {
+  if constexpr (S < SH::X::npass) {
+    x_pass<SH, S, -1>(sm, tw);
+    __syncthreads();
+    x_forward_from<SH, S + 1>(sm, tw);
+  }
+}
+
+template <class SH, int S>
+__device__ __forceinline__ void x_inverse_down_to(float2* sm, const float2* tw) {
+  // inverse passes npass-1 .. S (inclusive)
+  if constexpr (S < SH::X::npass) {
+    x_inverse_down_to<SH, S + 1>(sm, tw);
+    x_pass<SH, S, +1>(sm, tw);
+    __syncthreads();
+  }
+}
+
+// First x pass straight from HBM through the prologue.
+template <class SH, class Pro>
+__device__ __forceinline__ void x_first(float2* sm, const Pro& pro, int z, int y0base,
+                                        const float2* __restrict__ tw) {
+  using X = typename SH::X;
+  constexpr int R = X::radix(0), span = X::span(0), total = SH::ROWS * span;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int r = f / span;
+    const int i = f - r * span;
+    const int g = r / SH::AY, j = r - g * SH::AY;
+    const int y = y0base + g + SH::BY * j;
+    float2 v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = pro.load_c(i + t * span, y, z);
+    dft<R, -1>(v);
+    if (i != 0) {
+#pragma unroll
+      for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k]));
+    }
+    float2* row = sm + r * SH::ROWSTRIDE;
+#pragma unroll
+    for (int t = 0; t < R; ++t) row[xp<SH>(i + t * span)] = v[t];
+  }
+}
+
+// Last inverse x pass (pass 0) into the epilogue; FUSE re-applies forward
+// pass 0 to what the epilogue returns.
+template <class SH, class Epi, bool FUSE>
+__device__ __forceinline__ void x_last(float2* sm, Epi& epi, int z, int y0base,
+                                       const float2* __restrict__ tw) {
+  using X = typename SH::X;
+  constexpr int R = X::radix(0), span = X::span(0), total = SH::ROWS * span;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int r = f / span;
+    const int i = f - r * span;
+    const int g = r / SH::AY, j = r - g * SH::AY;
+    const int y = y0base + g + SH::BY * j;
+    float2* row = sm + r * SH::ROWSTRIDE;
+    float2 v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = row[xp<SH>(i + t * span)];
+    if (i != 0) {
+#pragma unroll
+      for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k]));
+    }
+    dft<R, +1>(v);
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = epi.apply_c(i + t * span, y, z, v[t]);
+    if constexpr (FUSE) {
+      dft<R, -1>(v);
+      if (i != 0) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k]));
+      }
+#pragma unroll
+      for (int t = 0; t < R; ++t) row[xp<SH>(i + t * span)] = v[t];
+    }
+  }
+}
+
+// ------------------------------------------------------- r2c / c2r columns
+template <class SH>
+__device__ __forceinline__ void split_store(float2* v, float2* __restrict__ S, int kx,
+                                            int z, int y0, const float2* __restrict__ twny) {
+  dft<SH::AY, -1>(v);
+#pragma unroll
+  for (int k1 = 0; k1 < SH::AY; ++k1) {
+    const float2 w = (k1 == 0 || y0 == 0) ? make_float2(1.f, 0.f) : __ldg(&twny[y0 * k1]);
+    S[sidx<SH>(k1, kx, z, y0)] = cmul(v[k1], w);
+  }
+}
+
+template <class SH>
+__device__ __forceinline__ void split_load(float2* v, const float2* __restrict__ S, int kx,
+                                           int z, int y0, const float2* __restrict__ twny) {
+#pragma unroll
+  for (int k1 = 0; k1 < SH::AY; ++k1) {
+    float2 a = __ldg(&S[sidx<SH>(k1, kx, z, y0)]);
+    if (k1 != 0 && y0 != 0) a = cmulc(a, __ldg(&twny[y0 * k1]));
+    v[k1] = a;
+  }
+  dft<SH::AY, +1>(v);
+}
+
+template <class SH>
+__device__ __forceinline__ void cols_forward(const float2* sm, float2* __restrict__ S, int z,
+                                             int y0base, const float2* __restrict__ twr,
+                                             const float2* __restrict__ twny) {
+  constexpr int M = SH::M, AY = SH::AY, RS = SH::ROWSTRIDE;
+  constexpr int total = SH::G * SH::ITEMS;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int g = f % SH::G;
+    const int it = f / SH::G;
+    const int y0 = y0base + g;
+    const float2* rows = sm + (g * AY) * RS;
+    if (it == 0) {
+      const int p0 = xp<SH>(0);
+#pragma unroll 1
+      for (int side = 0; side < 2; ++side) {
+        float2 xc[AY];
+#pragma unroll
+        for (int j = 0; j < AY; ++j) {
+          const float2 Z0 = rows[j * RS + p0];
+          xc[j] = make_float2(side == 0 ? Z0.x + Z0.y : Z0.x - Z0.y, 0.f);
+        }
+        split_store<SH>(xc, S, side == 0 ? 0 : M, z, y0, twny);
+      }
+      if constexpr (M % 2 == 0 && M >= 2) {
+        const int ph = xp<SH>(xrev<SH>(M / 2));
+        float2 xh[AY];
+#pragma unroll
+        for (int j = 0; j < AY; ++j) xh[j] = conjf2(rows[j * RS + ph]);
+        split_store<SH>(xh, S, M / 2, z, y0, twny);
+      }
+    } else {
+      const int k = it;
+      const int pa = xp<SH>(xrev<SH>(k));
+      const int pb = xp<SH>(xrev<SH>(M - k));
+      const float2 w = __ldg(&twr[k]);
+#pragma unroll 1
+      for (int side = 0; side < 2; ++side) {
+        float2 xc[AY];
+#pragma unroll
+        for (int j = 0; j < AY; ++j) {
+          const float2 a = rows[j * RS + pa];
+          const float2 b = conjf2(rows[j * RS + pb]);
+          const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
+          const float2 d = csub(a, b);
+          const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+          const float2 wo = cmul(w, o);
+          xc[j] = side == 0 ? cadd(e, wo) : conjf2(csub(e, wo));
+        }
+        split_store<SH>(xc, S, side == 0 ? k : M - k, z, y0, twny);
+      }
+    }
+  }
+}
+
+template <class SH>
+__device__ __forceinline__ void cols_inverse(float2* sm, const float2* __restrict__ S, int z,
+                                             int y0base, const float2* __restrict__ twr,
+                                             const float2* __restrict__ twny) {
+  constexpr int M = SH::M, AY = SH::AY, RS = SH::ROWSTRIDE;
+  constexpr int total = SH::G * SH::ITEMS;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int g = f % SH::G;
+    const int it = f / SH::G;
+    const int y0 = y0base + g;
+    float2* rows = sm + (g * AY) * RS;
+    if (it == 0) {
+      const int p0 = xp<SH>(0);
+      {
+        float2 xc[AY];
+        split_load<SH>(xc, S, 0, z, y0, twny);
+#pragma unroll
+        for (int j = 0; j < AY; ++j) rows[j * RS + p0] = xc[j];
+      }
+      {
+        float2 xm[AY];
+        split_load<SH>(xm, S, M, z, y0, twny);
+#pragma unroll
+        for (int j = 0; j < AY; ++j) {
+          const float x0 = rows[j * RS + p0].x;
+          rows[j * RS + p0] = make_float2(x0 + xm[j].x, x0 - xm[j].x);
+        }
+      }
+      if constexpr (M % 2 == 0 && M >= 2) {
+        float2 xh[AY];
+        split_load<SH>(xh, S, M / 2, z, y0, twny);
+        const int ph = xp<SH>(xrev<SH>(M / 2));
+#pragma unroll
+        for (int j = 0; j < AY; ++j) rows[j * RS + ph] = make_float2(2.f * xh[j].x, -2.f * xh[j].y);
+      }
+    } else {
+      const int k = it;
+      const int pa = xp<SH>(xrev<SH>(k));
+      const int pb = xp<SH>(xrev<SH>(M - k));
+      {
+        float2 xc[AY];
+        split_load<SH>(xc, S, k, z, y0, twny);
+#pragma unroll
+        for (int j = 0; j < AY; ++j) rows[j * RS + pa] = xc[j];
+      }
+      {
+        float2 xc[AY];
+        split_load<SH>(xc, S, M - k, z, y0, twny);
+#pragma unroll
+        for (int j = 0; j < AY; ++j) rows[j * RS + pb] = xc[j];
+      }
+      const float2 w = __ldg(&twr[k]);
+#pragma unroll 4
+      for (int j = 0; j < AY; ++j) {
+        const float2 xa = rows[j * RS + pa];
+        const float2 b = conjf2(rows[j * RS + pb]);
+        const float2 e = cadd(xa, b);
+        const float2 o = cmulc(csub(xa, b), w);
+        rows[j * RS + pa] = make_float2(e.x - o.y, e.y + o.x);
+        rows[j * RS + pb] = make_float2(e.x + o.y, -e.y + o.x);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ Z tile passes
+// y0 axis: lines (z, ki), element stride W; z axis: lines (y0, ki) = BW
+// contiguous lines, element stride BW.
+template <class SH, class A, int S, int DIR, bool ZAXIS>
+__device__ __forceinline__ void z_tile_pass(float2* sm, const float2* __restrict__ tw) {
+  constexpr int R = A::radix(S), len = A::len(S), span = len / R;
+  constexpr int per_line = A::n / R, twstep = A::n / len;
+  constexpr int nlines = ZAXIS ? SH::BW : SH::NZ * SH::W;
+  constexpr int l0n = ZAXIS ? SH::BW : SH::W;       // lines adjacent in memory
+  constexpr int es = ZAXIS ? SH::BW : SH::W;
+  constexpr int s1 = ZAXIS ? 0 : SH::BW;
+  constexpr int total = nlines * per_line;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int l0 = f % l0n;
+    const int rest = f / l0n;
+    const int rem = rest % per_line;
+    const int l1 = rest / per_line;
+    const int b = rem / span;
+    const int i = rem - b * span;
+    const int base = l1 * s1 + l0 + (b * len + i) * es;
+    float2 v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = sm[base + t * span * es];
+    if constexpr (DIR < 0) {
+      dft<R, -1>(v);
+      if (span > 1 && i != 0) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k * twstep]));
+      }
+    } else {
+      if (span > 1 && i != 0) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k * twstep]));
+      }
+      dft<R, +1>(v);
+    }
+#pragma unroll
+    for (int t = 0; t < R; ++t) sm[base + t * span * es] = v[t];
+  }
+}
+
+template <class SH, class A, int S, bool ZAXIS>
+__device__ __forceinline__ void tile_forward_from(float2* sm, const float2* tw) {
+  if constexpr (S < A::npass) {
+    z_tile_pass<SH, A, S, -1, ZAXIS>(sm, tw);
+    __syncthreads();
+    tile_forward_from<SH, A, S + 1, ZAXIS>(sm, tw);
+  }
+}
+template <class SH, class A, int S, bool ZAXIS>
+__device__ __forceinline__ void tile_inverse_down_to(float2* sm, const float2* tw) {
+  if constexpr (S < A::npass) {
+    tile_inverse_down_to<SH, A, S + 1, ZAXIS>(sm, tw);
+    z_tile_pass<SH, A, S, +1, ZAXIS>(sm, tw);
+    __syncthreads();
+  }
+}
+
+// Last forward z pass, spectral operation, first inverse z pass: one
+// register pass (the last DIF pass has span 1, so neither side needs
+// twiddles).
+template <class SH, class Mod>
+__device__ __forceinline__ void z_mod_pass(float2* sm, const Mod& mod, long long gbase) {
+  using A = typename SH::Z;
+  constexpr int S = A::npass - 1;
+  constexpr int R = A::radix(S);
+  constexpr int nblk = A::n / R;
+  constexpr int total = SH::BW * nblk;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int l0 = f % SH::BW;
+    const int b = f / SH::BW;
+    const int base = l0 + b * R * SH::BW;
+    float2 v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = sm[base + t * SH::BW];
+    dft<R, -1>(v);
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = mod.apply(gbase + base + t * SH::BW, v[t]);
+    dft<R, +1>(v);
+#pragma unroll
+    for (int t = 0; t < R; ++t) sm[base + t * SH::BW] = v[t];
+  }
+}
+
+struct Tables {
+  const float2* twx;   // w_M
+  const float2* twy;   // w_By
+  const float2* twz;   // w_nz
+  const float2* twr;   // w_nx (r2c split)
+  const float2* twny;  // w_ny (y split)
+};
+
+// ----------------------------------------------------------------- kernels
+template <class SH, class Pro>
+__global__ void __launch_bounds__(256, 2)
+    ks_xy_forward(const Pro pro, float2* __restrict__ S, const Tables T) {
+  CLARITY_DYN_SMEM(float2, sm);
+  const int z = blockIdx.x / SH::NGROUPS;
+  const int y0base = (blockIdx.x - z * SH::NGROUPS) * SH::G;
+  x_first<SH>(sm, pro, z, y0base, T.twx);
+  __syncthreads();
+  x_forward_from<SH, 1>(sm, T.twx);
+  cols_forward<SH>(sm, S, z, y0base, T.twr, T.twny);
+  pro.finish();
+}
+
+template <class SH, class Epi>
+__global__ void __launch_bounds__(256, 2)
+    ks_xy_inverse(Epi epi, const float2* __restrict__ S, const Tables T) {
+  CLARITY_DYN_SMEM(float2, sm);
+  const int z = blockIdx.x / SH::NGROUPS;
+  const int y0base = (blockIdx.x - z * SH::NGROUPS) * SH::G;
+  cols_inverse<SH>(sm, S, z, y0base, T.twr, T.twny);
+  __syncthreads();
+  x_inverse_down_to<SH, 1>(sm, T.twx);
+  x_last<SH, Epi, false>(sm, epi, z, y0base, T.twx);
+  epi.finish();
+}
+
+template <class SH, class Mid>
+__global__ void __launch_bounds__(256, 2)
+    ks_xy_inv_fwd(Mid mid, float2* __restrict__ S, const Tables T) {
+  CLARITY_DYN_SMEM(float2, sm);
+  const int z = blockIdx.x / SH::NGROUPS;
+  const int y0base = (blockIdx.x - z * SH::NGROUPS) * SH::G;
+  cols_inverse<SH>(sm, S, z, y0base, T.twr, T.twny);
+  __syncthreads();
+  x_inverse_down_to<SH, 1>(sm, T.twx);
+  x_last<SH, Mid, true>(sm, mid, z, y0base, T.twx);
+  __syncthreads();
+  x_forward_from<SH, 1>(sm, T.twx);
+  cols_forward<SH>(sm, S, z, y0base, T.twr, T.twny);
+  mid.finish();
+}
+
+template <class SH, class Mod>
+__global__ void __launch_bounds__(256, 2)
+    ks_z(const Mod mod, const float2* __restrict__ Sin, float2* __restrict__ Sout,
+         const Tables T) {
+  CLARITY_DYN_SMEM(float2, sm);
+  constexpr int tile = SH::TILE;
+  const long long base = (long long)blockIdx.x * tile;
+  static_assert(tile % 2 == 0, "tile must be even");
+  {
+    const float4* src = reinterpret_cast<const float4*>(Sin + base);
+    float4* dst = reinterpret_cast<float4*>(sm);
+#pragma unroll 4
+    for (int t = threadIdx.x; t < tile / 2; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) dst[t] = __ldg(&src[t]);
+  }
+  __syncthreads();
+  tile_forward_from<SH, typename SH::Y, 0, false>(sm, T.twy);
+  if constexpr (Mod::forward_only) {
+    tile_forward_from<SH, typename SH::Z, 0, true>(sm, T.twz);
+  } else {
+    // all z passes but the last, then last + spectral op + first inverse
+    if constexpr (SH::Z::npass >= 2) {
+      z_tile_pass<SH, typename SH::Z, 0, -1, true>(sm, T.twz);
+      __syncthreads();
+    }
+    if constexpr (SH::Z::npass >= 3) {
+      z_tile_pass<SH, typename SH::Z, 1, -1, true>(sm, T.twz);
+      __syncthreads();
+    }
+    z_mod_pass<SH>(sm, mod, base);
+    __syncthreads();
+    if constexpr (SH::Z::npass >= 3) {
+      z_tile_pass<SH, typename SH::Z, 1, +1, true>(sm, T.twz);
+      __syncthreads();
+    }
+    if constexpr (SH::Z::npass >= 2) {
+      z_tile_pass<SH, typename SH::Z, 0, +1, true>(sm, T.twz);
+      __syncthreads();
+    }
+    tile_inverse_down_to<SH, typename SH::Y, 0, false>(sm, T.twy);
+  }
+  {
+    float4* dst = reinterpret_cast<float4*>(Sout + base);
+    const float4* src = reinterpret_cast<const float4*>(sm);
+#pragma unroll 4
+    for (int t = threadIdx.x; t < tile / 2; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) dst[t] = src[t];
+  }
+}
+
+// Does a runtime plan match shape SH exactly (same radices and tiling)?
+template <class SH>
+inline bool matches(const VolPlan& P) {
+  auto same_axis = [](const AxisPlan& A, auto rad) {
+    using R = decltype(rad);
+    if (A.n != R::n || A.npass != R::npass) return false;
+    for (int s = 0; s < A.npass; ++s)
+      if (A.radix[s] != R::radix(s)) return false;
+    return true;
+  };
+  return P.xmode == 0 && P.M == SH::M && P.Ay == SH::AY && P.By == SH::BY &&
+         P.nz == SH::NZ && P.G == SH::G && P.W == SH::W && P.rowStride == SH::ROWSTRIDE &&
+         P.padShift == SH::PADSHIFT && same_axis(P.ax, typename SH::X{}) &&
+         same_axis(P.ayB, typename SH::Y{}) && same_axis(P.az, typename SH::Z{});
+}
+
+}  // namespace st
+}  // namespace clarity

@@ -1,0 +1,114 @@
+// static_dispatch.cuh -- compile-time specialised shapes and the launch
+// helpers that use them when a plan matches (else the generic kernels run).
+//
+// Shapes (work box x*y*z -> x radices, Ay, y0 radices, z radices, G, W),
+// exactly the plans the planner produces for these boxes:
+//   512x512x128   (256x256x64 image + same-size PSF): 16.16, 16, 8.4, 16.8, 2, 2
+//   128x128x64    (64x64x32 image + same-size PSF):   8.8,   16, 8,   8.8,  1, 4
+//   1024x1024x256 (512x512x128 image + PSF):          8.8.8, 16, 8.8, 16.16, 2, 1
+//   64x64x32      (small test box):                  8.4,   16, 4,   8.4,  4, 1
+#pragma once
+#include "engine.hpp"
+#include "ops.cuh"
+#include "passes_static.cuh"
+
+namespace clarity {
+
+using ShapeW512 = st::Shape<st::Rad<16, 16>, 16, st::Rad<8, 4>, st::Rad<16, 8>, 2, 2>;
+using ShapeW128 = st::Shape<st::Rad<8, 8>, 16, st::Rad<8>, st::Rad<8, 8>, 1, 4>;
+using ShapeW1024 = st::Shape<st::Rad<8, 8, 8>, 16, st::Rad<8, 8>, st::Rad<16, 16>, 2, 1>;
+using ShapeW64 = st::Shape<st::Rad<8, 4>, 16, st::Rad<4>, st::Rad<8, 4>, 4, 1>;
+
+template <class... SHs>
+struct ShapeList {};
+using StaticShapes = ShapeList<ShapeW512, ShapeW128, ShapeW1024, ShapeW64>;
+
+inline st::Tables tables_of(const PlanEntry& pe) {
+  const VolPlan& P = pe.P;
+  return st::Tables{pe.tw + P.ax.tw_off, pe.tw + P.ayB.tw_off, pe.tw + P.az.tw_off,
+                    pe.tw + P.tw_r2c_off, pe.tw + P.tw_ny_off};
+}
+
+template <class K>
+inline cudaError_t allow_smem_st(K kernel, int smem) {
+  if (smem > 48 * 1024)
+    return cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return cudaSuccess;
+}
+
+// Kernel families that may use the specialised kernels: bit KIND of the
+// CLARITY_STATIC environment variable (default: all).  Clearing bits selects
+// the runtime-generic kernels, which tests use to cover both paths.
+int static_family_mask();
+
+// kind: 0 xy forward, 1 z, 2 xy inverse+forward, 3 xy inverse
+template <class SH, int KIND, class F>
+inline bool try_static(const PlanEntry& pe, cudaStream_t st, const F& fn, float2* Sa,
+                       const float2* Sb, cudaError_t* err) {
+  if (!(static_family_mask() & (1 << KIND))) return false;
+  if (!st::matches<SH>(pe.P)) return false;
+  const st::Tables T = tables_of(pe);
+  if constexpr (KIND == 0) {
+    auto k = st::ks_xy_forward<SH, F>;
+    *err = allow_smem_st(k, SH::XY_SMEM);
+    if (*err != cudaSuccess) return true;
+    note_launch_begin(KK_XY_FORWARD, st);
+    CLARITY_LAUNCH(k, pe.P.xy_blocks, SH::THREADS, SH::XY_SMEM, st)(fn, Sa, T);
+    note_launch_end(KK_XY_FORWARD, st);
+  } else if constexpr (KIND == 1) {
+    auto k = st::ks_z<SH, F>;
+    *err = allow_smem_st(k, SH::Z_SMEM);
+    if (*err != cudaSuccess) return true;
+    note_launch_begin(KK_Z, st);
+    CLARITY_LAUNCH(k, pe.P.z_blocks, SH::THREADS, SH::Z_SMEM, st)(fn, Sb, Sa, T);
+    note_launch_end(KK_Z, st);
+  } else if constexpr (KIND == 2) {
+    auto k = st::ks_xy_inv_fwd<SH, F>;
+    *err = allow_smem_st(k, SH::XY_SMEM);
+    if (*err != cudaSuccess) return true;
+    note_launch_begin(KK_XY_INV_FWD, st);
+    CLARITY_LAUNCH(k, pe.P.xy_blocks, SH::THREADS, SH::XY_SMEM, st)(fn, Sa, T);
+    note_launch_end(KK_XY_INV_FWD, st);
+  } else {
+    auto k = st::ks_xy_inverse<SH, F>;
+    *err = allow_smem_st(k, SH::XY_SMEM);
+    if (*err != cudaSuccess) return true;
+    note_launch_begin(KK_XY_INVERSE, st);
+    CLARITY_LAUNCH(k, pe.P.xy_blocks, SH::THREADS, SH::XY_SMEM, st)(fn, Sb, T);
+    note_launch_end(KK_XY_INVERSE, st);
+  }
+  *err = cudaGetLastError();
+  return true;
+}
+
+template <int KIND, class F, class... SHs>
+inline bool try_static_all(ShapeList<SHs...>, const PlanEntry& pe, cudaStream_t st,
+                           const F& fn, float2* Sa, const float2* Sb, cudaError_t* err) {
+  return (try_static<SHs, KIND>(pe, st, fn, Sa, Sb, err) || ...);
+}
+
+// Entry points used by launch.cuh; each returns true when a specialised
+// kernel was launched (the error, if any, in *err).
+template <class F>
+bool static_xy_forward(const PlanEntry& pe, cudaStream_t st, const F& f, float2* S,
+                       cudaError_t* err) {
+  return try_static_all<0>(StaticShapes{}, pe, st, f, S, nullptr, err);
+}
+template <class F>
+bool static_z(const PlanEntry& pe, cudaStream_t st, const F& f, const float2* Sin,
+              float2* Sout, cudaError_t* err) {
+  return try_static_all<1>(StaticShapes{}, pe, st, f, Sout, Sin, err);
+}
+template <class F>
+bool static_xy_inv_fwd(const PlanEntry& pe, cudaStream_t st, const F& f, float2* S,
+                       cudaError_t* err) {
+  return try_static_all<2>(StaticShapes{}, pe, st, f, S, nullptr, err);
+}
+template <class F>
+bool static_xy_inverse(const PlanEntry& pe, cudaStream_t st, const F& f, const float2* S,
+                       cudaError_t* err) {
+  return try_static_all<3>(StaticShapes{}, pe, st, f, nullptr, S, err);
+}
+
+}  // namespace clarity
