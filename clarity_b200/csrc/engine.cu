@@ -381,6 +381,10 @@ static PaddedSrc padded(const float* src, Dims sd, Dims wd, int sx, int sy,
   return p;
 }
 
+static ImageSrc image_src(const float* src, Dims sd) {
+  return ImageSrc{src, sd.x, sd.y, sd.z};
+}
+
 static Dims work_dims(Dims id, Dims kd) {
   return Dims{id.x + kd.x, id.y + kd.y, id.z + kd.z};
 }
@@ -430,7 +434,7 @@ Status run_convolve(Context& ctx, const float* img, Dims id, const float* ker,
   CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
   const VolPlan& P = pe->P;
   CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
-  ProPadded pro{padded(img, id, wd, 0, 0, 0), nullptr, P.xmode};
+  ProImage pro{image_src(img, id), P.xmode};
   CL_TRY(xy_forward(ctx, *pe, pro, ws->S));
   CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, inv_volume(wd)}, ws->S, ws->S));
   EpiClip epi{out, id.x, id.y, id.z, nullptr, P.xmode};
@@ -446,7 +450,7 @@ Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
   CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
   const VolPlan& P = pe->P;
   CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
-  ProPadded pro{padded(img, id, wd, 0, 0, 0), nullptr, P.xmode};
+  ProImage pro{image_src(img, id), P.xmode};
   CL_TRY(xy_forward(ctx, *pe, pro, ws->S));
   CL_TRY(z_pass(ctx, *pe, ModWiener{ws->H, eps, inv_volume(wd)}, ws->S, ws->S));
   EpiClip epi{out, id.x, id.y, id.z, nullptr, P.xmode};
@@ -466,7 +470,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
                       bool rescale) {
   const VolPlan& P = pe.P;
   cudaStream_t st = ctx.exec_stream();
-  const PaddedSrc g = padded(img, id, wd, 0, 0, 0);
+  const ImageSrc g = image_src(img, id);
   const WorkVol wv{wd.x, wd.y, wd.z};
   const float scale_n = inv_volume(wd);
   float* sdev = ws.fscal;  // deferred flux scale
@@ -475,7 +479,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     const bool first = (k == 0);
     const float* cur_scale = (first || !rescale) ? nullptr : sdev;
     if (first) {
-      CL_TRY(xy_forward(ctx, pe, ProPadded{g, nullptr, P.xmode}, ws.S));
+      CL_TRY(xy_forward(ctx, pe, ProImage{g, P.xmode}, ws.S));
     } else {
       CL_TRY(xy_forward(ctx, pe, ProWork{ws.u, cur_scale, wv, P.xmode}, ws.S));
     }
@@ -577,11 +581,11 @@ Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
   CL_CHECK(cudaMemcpyAsync(hc, ws->fscal + 4, sizeof(hc), cudaMemcpyDeviceToHost, st));
   CL_CHECK(cudaStreamSynchronize(st));
   CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
-  const PaddedSrc g = padded(img, id, wd, 0, 0, 0);
+  const ImageSrc g = image_src(img, id);
   const WorkVol wv{wd.x, wd.y, wd.z};
   const float scale_n = inv_volume(wd);
   const int total = iters > 1 ? iters : 1;
-  CL_TRY(xy_forward(ctx, *pe, ProPadded{g, nullptr, P.xmode}, ws->S));
+  CL_TRY(xy_forward(ctx, *pe, ProImage{g, P.xmode}, ws->S));
   for (int k = 0; k < total; ++k) {
     CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, scale_n}, ws->S, ws->S));
     EpiJVC epi{k == 0 ? nullptr : ws->u, g, ws->u, hc[0], hc[1], wv, P.xmode};

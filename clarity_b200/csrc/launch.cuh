@@ -111,6 +111,8 @@ Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
                                              const ProWork&, float2*);              \
   extern template Status xy_forward<ProPadded>(Context&, const PlanEntry&,          \
                                                const ProPadded&, float2*);          \
+  extern template Status xy_forward<ProImage>(Context&, const PlanEntry&,           \
+                                              const ProImage&, float2*);            \
   extern template Status xy_inverse<EpiClip>(Context&, const PlanEntry&,            \
                                              const EpiClip&, const float2*);        \
   extern template Status xy_inverse<EpiWork>(Context&, const PlanEntry&,            \

@@ -155,20 +155,18 @@ extern "C" CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
   pk.X = kernelDim.x; pk.Y = kernelDim.y; pk.Z = kernelDim.z;
   pk.sx = -kernelDim.x / 2; pk.sy = -kernelDim.y / 2; pk.sz = -kernelDim.z / 2;
   pk.nx = nx; pk.ny = ny; pk.nz = nz;
-  PaddedSrc pi = pk;
-  pi.src = image;
-  pi.X = imageDim.x; pi.Y = imageDim.y; pi.Z = imageDim.z;
-  pi.sx = pi.sy = pi.sz = 0;
   const ProPadded pro_k{pk, nullptr, P.xmode};
-  const ProPadded pro_i{pi, nullptr, P.xmode};
+  const ProImage pro_i{ImageSrc{image, imageDim.x, imageDim.y, imageDim.z}, P.xmode};
   const ModOTF mod{H, 1.0f / ((float)wd.z * wd.y * wd.x)};
   const EpiClip epi{out, imageDim.x, imageDim.y, imageDim.z, nullptr, P.xmode};
 
   auto kf = k_xy_forward<ProPadded>;
+  auto kfi = k_xy_forward<ProImage>;
   auto kzf = k_z<ModForward>;
   auto kzm = k_z<ModOTF>;
   auto ki = k_xy_inverse<EpiClip>;
   if ((e = allow_smem(kf, P.xy_smem)) != cudaSuccess ||
+      (e = allow_smem(kfi, P.xy_smem)) != cudaSuccess ||
       (e = allow_smem(kzf, P.z_smem)) != cudaSuccess ||
       (e = allow_smem(kzm, P.z_smem)) != cudaSuccess ||
       (e = allow_smem(ki, P.xy_smem)) != cudaSuccess)
@@ -176,7 +174,7 @@ extern "C" CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
   // OTF of the shifted kernel, then R2C(image) * OTF / N, then C2R + clip
   CLARITY_LAUNCH(kf, P.xy_blocks, P.xy_threads, P.xy_smem, st)(P, pro_k, H, tw, xrev);
   CLARITY_LAUNCH(kzf, P.z_blocks, P.z_threads, P.z_smem, st)(P, ModForward{}, H, H, tw);
-  CLARITY_LAUNCH(kf, P.xy_blocks, P.xy_threads, P.xy_smem, st)(P, pro_i, S, tw, xrev);
+  CLARITY_LAUNCH(kfi, P.xy_blocks, P.xy_threads, P.xy_smem, st)(P, pro_i, S, tw, xrev);
   CLARITY_LAUNCH(kzm, P.z_blocks, P.z_threads, P.z_smem, st)(P, mod, S, S, tw);
   CLARITY_LAUNCH(ki, P.xy_blocks, P.xy_threads, P.xy_smem, st)(P, epi, S, tw, xrev);
   e = cudaGetLastError();

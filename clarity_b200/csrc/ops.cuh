@@ -23,11 +23,24 @@ __device__ __forceinline__ float rl_ratio(float g, float b) {
   return (fabsf(b) <= 1e-5f) ? 0.f : g / b;
 }
 
-// Real volume on the padded work box, x fastest.
+// Real volume on the padded work box, x fastest.  The planner rejects boxes
+// of 2^31 voxels or more, so 32-bit offsets suffice.
 struct WorkVol {
   int nx, ny, nz;
-  __device__ __forceinline__ long long idx(int x, int y, int z) const {
-    return ((long long)z * ny + y) * nx + x;
+  __device__ __forceinline__ unsigned idx(int x, int y, int z) const {
+    return ((unsigned)z * ny + y) * nx + x;
+  }
+};
+
+// Unpadded image seen on the work box with zero shift
+// (src/MaximumLikelihoodDeconvolve.cxx:278-282): the image itself inside
+// [0,X)x[0,Y)x[0,Z), zero in the padding.  Only bounds checks, no modulo.
+struct ImageSrc {
+  const float* __restrict__ src;
+  int X, Y, Z;
+  __device__ __forceinline__ float at(int x, int y, int z) const {
+    if (x < X && y < Y && z < Z) return __ldg(&src[((unsigned)z * Y + y) * X + x]);
+    return 0.f;
   }
 };
 
@@ -90,6 +103,17 @@ struct ProPadded {
     float a = p.at(m, y, z);
     if (scale) a = s * a;
     return make_float2(a, 0.f);
+  }
+  __device__ __forceinline__ void finish() const {}
+};
+
+// The padded image (zero shift) as a prologue.
+struct ProImage {
+  ImageSrc p;
+  int xmode;
+  __device__ __forceinline__ float2 load_c(int m, int y, int z) const {
+    if (xmode == 0) return make_float2(p.at(2 * m, y, z), p.at(2 * m + 1, y, z));
+    return make_float2(p.at(m, y, z), 0.f);
   }
   __device__ __forceinline__ void finish() const {}
 };
@@ -159,7 +183,7 @@ struct EpiClip {
 // the first iteration), partial sums of u_new in FP64.
 struct EpiRLProduct {
   const float* __restrict__ cur;     // work-box estimate, or nullptr
-  PaddedSrc g;                       // used when cur == nullptr
+  ImageSrc g;                        // used when cur == nullptr
   const float* __restrict__ scale;   // deferred flux scale for cur
   float* __restrict__ unew;
   double* __restrict__ partial;
@@ -193,7 +217,7 @@ struct EpiRLProduct {
 // RL step 2 (src/MaximumLikelihoodDeconvolve.cxx:61-62): r = g / (h*u) with
 // the 1e-5 guard, fused between the inverse and forward transforms.
 struct MidRLRatio {
-  PaddedSrc g;
+  ImageSrc g;
   int xmode;
   __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 b) {
     if (xmode == 0)
@@ -211,7 +235,7 @@ struct MidRLRatio {
 // fused kernel transforms it for the next iteration.
 struct EpiJVC {
   const float* __restrict__ cur;
-  PaddedSrc g;
+  ImageSrc g;
   float* __restrict__ inext;
   float A, invASq;
   WorkVol w;

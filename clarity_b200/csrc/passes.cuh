@@ -181,10 +181,13 @@ __device__ __forceinline__ void x_load_only(float2* sm, const VolPlan& P,
 //   even mode: it == 0 handles kx = 0, M (and M/2 when M is even);
 //              it >= 1 handles the pair (it, M - it);
 //   odd mode:  item it is the single column kx = it.
-__device__ __forceinline__ long long s_index(const VolPlan& P, int k1, int kx,
-                                             int z, int y0) {
+// Offset of S[0][kg][z][y0][ki] (kx = kg*W + ki); k1 adds k1_stride(P).
+__device__ __forceinline__ unsigned s_base(const VolPlan& P, int kx, int z, int y0) {
   const int kg = kx / P.W, ki = kx - kg * P.W;
-  return ((((long long)k1 * P.KG + kg) * P.nz + z) * P.By + y0) * P.W + ki;
+  return (((unsigned)kg * P.nz + z) * P.By + y0) * P.W + ki;
+}
+__device__ __forceinline__ unsigned k1_stride(const VolPlan& P) {
+  return (unsigned)P.KG * P.nz * P.By * P.W;
 }
 
 template <int AY>
@@ -193,11 +196,13 @@ __device__ __forceinline__ void col_split_store(float2* v, const VolPlan& P,
                                                 int z, int y0,
                                                 const float2* __restrict__ twny) {
   dft<AY, -1>(v);
+  float2* dst = S + s_base(P, kx, z, y0);
+  const unsigned ks = k1_stride(P);
 #pragma unroll
   for (int k1 = 0; k1 < AY; ++k1) {
     float2 w = (k1 == 0 || y0 == 0) ? make_float2(1.f, 0.f)
                                     : __ldg(&twny[y0 * k1]);
-    S[s_index(P, k1, kx, z, y0)] = cmul(v[k1], w);
+    dst[k1 * ks] = cmul(v[k1], w);
   }
 }
 
@@ -278,9 +283,11 @@ __device__ __forceinline__ void col_split_load(float2* v, const VolPlan& P,
                                                const float2* __restrict__ S,
                                                int kx, int z, int y0,
                                                const float2* __restrict__ twny) {
+  const float2* src = S + s_base(P, kx, z, y0);
+  const unsigned ks = k1_stride(P);
 #pragma unroll
   for (int k1 = 0; k1 < AY; ++k1) {
-    float2 a = __ldg(&S[s_index(P, k1, kx, z, y0)]);
+    float2 a = __ldg(&src[k1 * ks]);
     if (k1 != 0 && y0 != 0) a = cmulc(a, __ldg(&twny[y0 * k1]));
     v[k1] = a;
   }

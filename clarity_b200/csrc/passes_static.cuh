@@ -51,6 +51,12 @@ struct Shape {
   static constexpr int XY_SMEM = ROWS * ROWSTRIDE * 8;
   static constexpr int Z_SMEM = TILE * 8;
   static constexpr int NGROUPS = BY / G;
+  // Z kernel with one register pass per y0 line (BY <= 32): padded z stride
+  // ZS = BW + W keeps both the per-line y0 accesses and the z passes free of
+  // bank conflicts.
+  static constexpr bool Y_PER_LINE = BY <= 32;
+  static constexpr int ZS = BW + W;
+  static constexpr int Z2_SMEM = NZ * ZS * 8;
 };
 
 template <class SH>
@@ -72,11 +78,14 @@ __device__ __forceinline__ int xrev(int k) {
   return pos;
 }
 
+// Offset of S[0][kg][z][y0][ki] for kx = kg*W + ki; k1 adds K1STRIDE.
 template <class SH>
-__device__ __forceinline__ long long sidx(int k1, int kx, int z, int y0) {
+__device__ __forceinline__ unsigned sbase(int kx, int z, int y0) {
   const int kg = kx / SH::W, ki = kx % SH::W;
-  return ((((long long)k1 * SH::KG + kg) * SH::NZ + z) * SH::BY + y0) * SH::W + ki;
+  return (((unsigned)kg * SH::NZ + z) * SH::BY + y0) * SH::W + ki;
 }
+template <class SH>
+constexpr unsigned kK1Stride = (unsigned)SH::KG * SH::NZ * SH::BY * SH::W;
 
 // ------------------------------------------------------------------ x rows
 // One register pass S of the x axis over all rows of the XY tile.
@@ -200,19 +209,21 @@ template <class SH>
 __device__ __forceinline__ void split_store(float2* v, float2* __restrict__ S, int kx,
                                             int z, int y0, const float2* __restrict__ twny) {
   dft<SH::AY, -1>(v);
+  float2* dst = S + sbase<SH>(kx, z, y0);
 #pragma unroll
   for (int k1 = 0; k1 < SH::AY; ++k1) {
     const float2 w = (k1 == 0 || y0 == 0) ? make_float2(1.f, 0.f) : __ldg(&twny[y0 * k1]);
-    S[sidx<SH>(k1, kx, z, y0)] = cmul(v[k1], w);
+    dst[k1 * kK1Stride<SH>] = cmul(v[k1], w);
   }
 }
 
 template <class SH>
 __device__ __forceinline__ void split_load(float2* v, const float2* __restrict__ S, int kx,
                                            int z, int y0, const float2* __restrict__ twny) {
+  const float2* src = S + sbase<SH>(kx, z, y0);
 #pragma unroll
   for (int k1 = 0; k1 < SH::AY; ++k1) {
-    float2 a = __ldg(&S[sidx<SH>(k1, kx, z, y0)]);
+    float2 a = __ldg(&src[k1 * kK1Stride<SH>]);
     if (k1 != 0 && y0 != 0) a = cmulc(a, __ldg(&twny[y0 * k1]));
     v[k1] = a;
   }
@@ -522,6 +533,136 @@ __global__ void __launch_bounds__(256, 2)
     const float4* src = reinterpret_cast<const float4*>(sm);
 #pragma unroll 4
     for (int t = threadIdx.x; t < tile / 2; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) dst[t] = src[t];
+  }
+}
+
+// ----------------------------------------------- Z kernel, y0 per line
+// z-axis register pass S over the padded tile: lines l0 < BW (adjacent in
+// memory), element e of line l0 at l0 + e*ZS.
+template <class SH, int S, int DIR>
+__device__ __forceinline__ void z2_pass(float2* sm, const float2* __restrict__ tw) {
+  using A = typename SH::Z;
+  constexpr int R = A::radix(S), len = A::len(S), span = len / R;
+  constexpr int per_line = A::n / R, twstep = A::n / len;
+  constexpr int total = SH::BW * per_line;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int l0 = f % SH::BW;
+    const int rem = f / SH::BW;
+    const int b = rem / span;
+    const int i = rem - b * span;
+    const int base = l0 + (b * len + i) * SH::ZS;
+    float2 v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = sm[base + t * span * SH::ZS];
+    if constexpr (DIR < 0) {
+      dft<R, -1>(v);
+      if (span > 1 && i != 0) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k * twstep]));
+      }
+    } else {
+      if (span > 1 && i != 0) {
+#pragma unroll
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k * twstep]));
+      }
+      dft<R, +1>(v);
+    }
+#pragma unroll
+    for (int t = 0; t < R; ++t) sm[base + t * span * SH::ZS] = v[t];
+  }
+}
+
+// Last z pass (span 1): forward DIF; then either the spectral operation and
+// the first inverse pass back to smem, or (forward only) a store of the
+// spectrum to HBM.  The global offset of tile element (z, l0) is
+// gbase + z*BW + l0.
+template <class SH, class Mod>
+__device__ __forceinline__ void z2_last(float2* sm, const Mod& mod, unsigned gbase,
+                                        float2* __restrict__ out) {
+  using A = typename SH::Z;
+  constexpr int S = A::npass - 1;
+  constexpr int R = A::radix(S);
+  constexpr int nblk = A::n / R;
+  constexpr int total = SH::BW * nblk;
+#pragma unroll 1
+  for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int l0 = f % SH::BW;
+    const int b = f / SH::BW;
+    const int sbase = l0 + b * R * SH::ZS;
+    const unsigned g0 = gbase + l0 + b * R * SH::BW;
+    float2 v[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) v[t] = sm[sbase + t * SH::ZS];
+    dft<R, -1>(v);
+    if constexpr (Mod::forward_only) {
+#pragma unroll
+      for (int t = 0; t < R; ++t) out[g0 + t * SH::BW] = v[t];
+    } else {
+#pragma unroll
+      for (int t = 0; t < R; ++t) v[t] = mod.apply(g0 + t * SH::BW, v[t]);
+      dft<R, +1>(v);
+#pragma unroll
+      for (int t = 0; t < R; ++t) sm[sbase + t * SH::ZS] = v[t];
+    }
+  }
+}
+
+template <class SH, class Mod>
+__global__ void __launch_bounds__(256, 2)
+    ks_z2(const Mod mod, const float2* __restrict__ Sin, float2* __restrict__ Sout,
+          const Tables T) {
+  CLARITY_DYN_SMEM(float2, sm);
+  static_assert(SH::Y_PER_LINE, "y0 per-line Z kernel needs BY <= 32");
+  constexpr int BY = SH::BY, W = SH::W, BW = SH::BW, NZ = SH::NZ, ZS = SH::ZS;
+  using A = typename SH::Z;
+  const unsigned gbase = blockIdx.x * (unsigned)SH::TILE;
+  // y0 forward, one line (z, ki) per thread, straight from HBM
+#pragma unroll 1
+  for (int l = threadIdx.x; l < NZ * W; l += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int ki = l % W, z = l / W;
+    const float2* src = Sin + gbase + z * BW + ki;
+    float2 v[BY];
+#pragma unroll
+    for (int y = 0; y < BY; ++y) v[y] = __ldg(&src[y * W]);
+    dft<BY, -1>(v);
+    float2* d = sm + z * ZS + ki;
+#pragma unroll
+    for (int k = 0; k < BY; ++k) d[k * W] = v[k];
+  }
+  __syncthreads();
+  if constexpr (A::npass >= 2) {
+    z2_pass<SH, 0, -1>(sm, T.twz);
+    __syncthreads();
+  }
+  if constexpr (A::npass >= 3) {
+    z2_pass<SH, 1, -1>(sm, T.twz);
+    __syncthreads();
+  }
+  z2_last<SH>(sm, mod, gbase, Sout);
+  if constexpr (!Mod::forward_only) {
+    __syncthreads();
+    if constexpr (A::npass >= 3) {
+      z2_pass<SH, 1, +1>(sm, T.twz);
+      __syncthreads();
+    }
+    if constexpr (A::npass >= 2) {
+      z2_pass<SH, 0, +1>(sm, T.twz);
+      __syncthreads();
+    }
+    // y0 inverse per line, straight to HBM
+#pragma unroll 1
+    for (int l = threadIdx.x; l < NZ * W; l += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+      const int ki = l % W, z = l / W;
+      const float2* d = sm + z * ZS + ki;
+      float2 v[BY];
+#pragma unroll
+      for (int k = 0; k < BY; ++k) v[k] = d[k * W];
+      dft<BY, +1>(v);
+      float2* dst = Sout + gbase + z * BW + ki;
+#pragma unroll
+      for (int y = 0; y < BY; ++y) dst[y * W] = v[y];
+    }
   }
 }
 

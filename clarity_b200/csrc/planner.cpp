@@ -145,6 +145,12 @@ bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
     return false;
   }
   P = best;
+  // 32-bit offsets address every real and spectral element
+  const long long spec = (long long)P.Ay * P.KG * P.nz * P.By * P.W;
+  if ((long long)nx * ny * nz >= (1ll << 31) || spec >= (1ll << 31)) {
+    if (why) *why = "work box of 2^31 voxels or more";
+    return false;
+  }
   P.xy_threads = 256;
   P.z_threads = 256;
   P.spec_elems = (long long)P.Ay * P.KG * P.nz * P.By * P.W;

@@ -57,12 +57,21 @@ inline bool try_static(const PlanEntry& pe, cudaStream_t st, const F& fn, float2
     CLARITY_LAUNCH(k, pe.P.xy_blocks, SH::THREADS, SH::XY_SMEM, st)(fn, Sa, T);
     note_launch_end(KK_XY_FORWARD, st);
   } else if constexpr (KIND == 1) {
-    auto k = st::ks_z<SH, F>;
-    *err = allow_smem_st(k, SH::Z_SMEM);
-    if (*err != cudaSuccess) return true;
-    note_launch_begin(KK_Z, st);
-    CLARITY_LAUNCH(k, pe.P.z_blocks, SH::THREADS, SH::Z_SMEM, st)(fn, Sb, Sa, T);
-    note_launch_end(KK_Z, st);
+    if constexpr (SH::Y_PER_LINE) {
+      auto k = st::ks_z2<SH, F>;
+      *err = allow_smem_st(k, SH::Z2_SMEM);
+      if (*err != cudaSuccess) return true;
+      note_launch_begin(KK_Z, st);
+      CLARITY_LAUNCH(k, pe.P.z_blocks, SH::THREADS, SH::Z2_SMEM, st)(fn, Sb, Sa, T);
+      note_launch_end(KK_Z, st);
+    } else {
+      auto k = st::ks_z<SH, F>;
+      *err = allow_smem_st(k, SH::Z_SMEM);
+      if (*err != cudaSuccess) return true;
+      note_launch_begin(KK_Z, st);
+      CLARITY_LAUNCH(k, pe.P.z_blocks, SH::THREADS, SH::Z_SMEM, st)(fn, Sb, Sa, T);
+      note_launch_end(KK_Z, st);
+    }
   } else if constexpr (KIND == 2) {
     auto k = st::ks_xy_inv_fwd<SH, F>;
     *err = allow_smem_st(k, SH::XY_SMEM);
