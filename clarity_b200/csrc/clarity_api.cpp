@@ -112,7 +112,7 @@ ClarityResult_t host_call(const float* in, Clarity_Dim3 id, const float* ker,
   e = cudaMemcpyAsync(out, g_stage.out, sizeof(float) * ni, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "device to host copy"));
-  return CLARITY_SUCCESS;
+  return report(ctx->check_device_errors());
 }
 
 template <class Run>

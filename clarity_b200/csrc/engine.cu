@@ -267,6 +267,7 @@ Context::~Context() {
   for (auto& kv : plans_) {
     cudaFree(kv.second->tw);
     cudaFree(kv.second->xrev);
+    cudaFree(kv.second->err);
   }
   plans_.clear();
   if (stream_) cudaStreamDestroy(stream_);
@@ -298,6 +299,8 @@ Status Context::plan(const Dims& wd, const PlanEntry** out) {
   const VolPlan& P = pe->P;
   CL_CHECK(dev_alloc((void**)&pe->tw, sizeof(float2) * P.twiddle_count));
   CL_CHECK(dev_alloc((void**)&pe->xrev, sizeof(int) * std::max(P.xrev_count, 1)));
+  CL_CHECK(dev_alloc((void**)&pe->err, sizeof(int)));
+  CL_CHECK(cudaMemsetAsync(pe->err, 0, sizeof(int), exec_stream()));
   std::vector<int> rev;
   std::vector<TwTable> tabs;
   plan_tables(P, &rev, &tabs);
@@ -314,6 +317,21 @@ Status Context::plan(const Dims& wd, const PlanEntry** out) {
   cudaFree(dtabs);
   *out = pe.get();
   plans_[key] = std::move(pe);
+  return Status::Ok();
+}
+
+Status Context::check_device_errors() {
+  for (auto& kv : plans_) {
+    int e = 0;
+    CL_CHECK(cudaMemcpy(&e, kv.second->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e != 0) {
+      CL_CHECK(cudaMemset(kv.second->err, 0, sizeof(int)));
+      Status s;
+      s.code = CLARITY_INVALID_OPERATION;
+      s.msg = "a device-side wait timed out (code " + std::to_string(e) + ")";
+      return s;
+    }
+  }
   return Status::Ok();
 }
 

@@ -37,6 +37,7 @@ struct PlanEntry {
   VolPlan P;
   float2* tw = nullptr;  // twiddle tables (FP64-generated, rounded)
   int* xrev = nullptr;   // natural x frequency -> smem slot after x passes
+  int* err = nullptr;    // device error word: nonzero after a bounded wait gave up
 };
 
 
@@ -72,6 +73,8 @@ class Context {
   Status workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
                    Workspace** out);
   void release_workspaces();
+  // Reads and clears every plan's device error word (synchronous).
+  Status check_device_errors();
 
   std::mutex mu;  // serialises API calls on this context
 

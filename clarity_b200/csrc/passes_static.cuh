@@ -10,6 +10,7 @@
 #include "dft_codelets.cuh"
 #include "launch_macro.cuh"
 #include "plan.hpp"
+#include "tma.cuh"
 
 namespace clarity {
 namespace st {
@@ -443,6 +444,7 @@ struct Tables {
   const float2* twz;   // w_nz
   const float2* twr;   // w_nx (r2c split)
   const float2* twny;  // w_ny (y split)
+  int* err;            // device error word (bounded waits that gave up)
 };
 
 // ----------------------------------------------------------------- kernels
@@ -615,18 +617,48 @@ __global__ void __launch_bounds__(256, 2)
   CLARITY_DYN_SMEM(float2, sm);
   static_assert(SH::Y_PER_LINE, "y0 per-line Z kernel needs BY <= 32");
   constexpr int BY = SH::BY, W = SH::W, BW = SH::BW, NZ = SH::NZ, ZS = SH::ZS;
+  // z rows of the tile are contiguous BW*8-byte runs in HBM and land at
+  // ZS*8-byte strides in shared memory: bulk copies when both are 16-byte
+  // multiples
+  constexpr bool BULK = (BW * 8) % 16 == 0 && (ZS * 8) % 16 == 0;
   using A = typename SH::Z;
   const unsigned gbase = blockIdx.x * (unsigned)SH::TILE;
-  // y0 forward, one line (z, ki) per thread, straight from HBM
+  __shared__ alignas(8) uint64_t bar;
+  if constexpr (BULK) {
+    static_assert((BW * 8) % 16 == 0 && (ZS * 8) % 16 == 0 && (SH::TILE * 8) % 16 == 0,
+                  "bulk copies need 16-byte sizes and offsets");
+    if (!smem_aligned16(sm)) {  // never expected: refuse rather than fault
+      if (threadIdx.x == 0) atomicExch(T.err, kErrMisaligned);
+      return;
+    }
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if ((int)threadIdx.x < CLARITY_ISSUE_LANES) {
+      if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, (uint32_t)(NZ * BW * 8));
+      __syncwarp();
+      for (int z = threadIdx.x; z < NZ; z += CLARITY_ISSUE_LANES)
+        bulk_load(sm + z * ZS, Sin + gbase + z * BW, BW * 8, &bar);
+    }
+    if (!mbar_wait(&bar, 0, T.err)) {
+      mbar_wait(&bar, 0, nullptr);  // give copies in flight a last chance
+      return;
+    }
+  }
+  // y0 forward, one line (z, ki) per thread
 #pragma unroll 1
   for (int l = threadIdx.x; l < NZ * W; l += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
     const int ki = l % W, z = l / W;
-    const float2* src = Sin + gbase + z * BW + ki;
     float2 v[BY];
-#pragma unroll
-    for (int y = 0; y < BY; ++y) v[y] = __ldg(&src[y * W]);
-    dft<BY, -1>(v);
     float2* d = sm + z * ZS + ki;
+    if constexpr (BULK) {
+#pragma unroll
+      for (int y = 0; y < BY; ++y) v[y] = d[y * W];
+    } else {
+      const float2* src = Sin + gbase + z * BW + ki;
+#pragma unroll
+      for (int y = 0; y < BY; ++y) v[y] = __ldg(&src[y * W]);
+    }
+    dft<BY, -1>(v);
 #pragma unroll
     for (int k = 0; k < BY; ++k) d[k * W] = v[k];
   }
@@ -650,18 +682,32 @@ __global__ void __launch_bounds__(256, 2)
       z2_pass<SH, 0, +1>(sm, T.twz);
       __syncthreads();
     }
-    // y0 inverse per line, straight to HBM
+    // y0 inverse per line
 #pragma unroll 1
     for (int l = threadIdx.x; l < NZ * W; l += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
       const int ki = l % W, z = l / W;
-      const float2* d = sm + z * ZS + ki;
+      float2* d = sm + z * ZS + ki;
       float2 v[BY];
 #pragma unroll
       for (int k = 0; k < BY; ++k) v[k] = d[k * W];
       dft<BY, +1>(v);
-      float2* dst = Sout + gbase + z * BW + ki;
+      if constexpr (BULK) {
 #pragma unroll
-      for (int y = 0; y < BY; ++y) dst[y * W] = v[y];
+        for (int y = 0; y < BY; ++y) d[y * W] = v[y];
+      } else {
+        float2* dst = Sout + gbase + z * BW + ki;
+#pragma unroll
+        for (int y = 0; y < BY; ++y) dst[y * W] = v[y];
+      }
+    }
+    if constexpr (BULK) {
+      fence_smem_to_async();
+      __syncthreads();
+      if ((int)threadIdx.x < CLARITY_ISSUE_LANES) {
+        for (int z = threadIdx.x; z < NZ; z += CLARITY_ISSUE_LANES)
+          bulk_store(Sout + gbase + z * BW, sm + z * ZS, BW * 8);
+        bulk_store_commit_and_wait();
+      }
     }
   }
 }

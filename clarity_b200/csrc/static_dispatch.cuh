@@ -26,7 +26,7 @@ using StaticShapes = ShapeList<ShapeW512, ShapeW128, ShapeW1024, ShapeW64>;
 inline st::Tables tables_of(const PlanEntry& pe) {
   const VolPlan& P = pe.P;
   return st::Tables{pe.tw + P.ax.tw_off, pe.tw + P.ayB.tw_off, pe.tw + P.az.tw_off,
-                    pe.tw + P.tw_r2c_off, pe.tw + P.tw_ny_off};
+                    pe.tw + P.tw_r2c_off, pe.tw + P.tw_ny_off, pe.err};
 }
 
 template <class K>

@@ -72,6 +72,7 @@ inline T __ldg(const T* p) {
 inline float __shfl_xor_sync(unsigned, float, int) { return 0.f; }
 inline double __shfl_xor_sync(unsigned, double, int) { return 0.0; }
 inline void __syncthreads() {}
+inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline void sincospi(double x, double* s, double* c) {
   *s = std::sin(M_PI * x);
   *c = std::cos(M_PI * x);

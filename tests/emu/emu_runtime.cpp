@@ -35,6 +35,18 @@ cudaError_t cudaStreamDestroy(cudaStream_t s) {
   return cudaSuccess;
 }
 cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
+cudaError_t cudaMemsetAsync(void* p, int v, size_t n, cudaStream_t) {
+  std::memset(p, v, n);
+  return cudaSuccess;
+}
+cudaError_t cudaMemset(void* p, int v, size_t n) {
+  std::memset(p, v, n);
+  return cudaSuccess;
+}
+cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) {
+  std::memcpy(d, s, n);
+  return cudaSuccess;
+}
 cudaError_t cudaDeviceSynchronize(void) { return cudaSuccess; }
 cudaError_t cudaSetDevice(int) { return cudaSuccess; }
 cudaError_t cudaGetDeviceCount(int* c) {
