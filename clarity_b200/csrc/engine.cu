@@ -476,13 +476,16 @@ Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
   return Status::Ok();
 }
 
-// Richardson-Lucy, five fused passes per iteration:
-//   P1 xy-forward of cur = s*u (or the padded image)      -> S
-//   P2 z pass: y0/z forward, * OTF / N, inverse           -> S   (h * cur)
+// Richardson-Lucy (src/MaximumLikelihoodDeconvolve.cxx:48-81), four fused
+// passes per iteration after a one-off forward transform of the image:
+//   P2 z pass: y0/z forward, * OTF * s/N, inverse        -> S   (h * cur)
 //   P3 xy inverse, r = g / (h*cur) with the 1e-5 guard, xy forward -> S
-//   P4 z pass again                                       -> S   (h * r)
-//   P5 xy inverse, u' = cur * (h*r), FP64 partial sums    -> u
-// then s = E / sum(u') on the device (deferred flux rescale).
+//   P4 z pass again                                      -> S   (h * r)
+//   P5 xy inverse, u' = cur * (h*r), FP64 partial sums, and (except on the
+//      last iteration) the xy forward transform of u'   -> u, S
+// then s = E / sum(u') on the device.  cur = s*u' is never stored: P5 reads
+// u' and s, and P2 of the next iteration applies s to the transform of u'
+// (the flux rescale of :73-78, deferred).
 static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
                       const float* img, Dims id, Dims wd, int iters,
                       bool rescale) {
@@ -493,31 +496,29 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
   const float scale_n = inv_volume(wd);
   float* sdev = ws.fscal;  // deferred flux scale
   if (rescale) CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
+  CL_TRY(xy_forward(ctx, pe, ProImage{g, P.xmode}, ws.S));
   for (int k = 0; k < iters; ++k) {
-    const bool first = (k == 0);
-    const float* cur_scale = (first || !rescale) ? nullptr : sdev;
-    if (first) {
-      CL_TRY(xy_forward(ctx, pe, ProImage{g, P.xmode}, ws.S));
-    } else {
-      CL_TRY(xy_forward(ctx, pe, ProWork{ws.u, cur_scale, wv, P.xmode}, ws.S));
-    }
-    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n}, ws.S, ws.S));
+    const float* sk = (k == 0 || !rescale) ? nullptr : sdev;
+    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n, sk}, ws.S, ws.S));
     CL_TRY(xy_inv_fwd(ctx, pe, MidRLRatio{g, P.xmode}, ws.S));
     CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n}, ws.S, ws.S));
     EpiRLProduct epi;
-    epi.cur = first ? nullptr : ws.u;
+    epi.cur = (k == 0) ? nullptr : ws.u;
     epi.g = g;
-    epi.scale = cur_scale;
+    epi.scale = sk;
     epi.unew = ws.u;
     epi.partial = ws.partial;
     epi.w = wv;
     epi.xmode = P.xmode;
     epi.acc = 0.0;
-    CL_TRY(xy_inverse(ctx, pe, epi, ws.S));
+    if (k + 1 < iters)
+      CL_TRY(xy_inv_fwd(ctx, pe, epi, ws.S));
+    else
+      CL_TRY(xy_inverse(ctx, pe, epi, ws.S));
     if (rescale) {
       count_small();
       CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws.partial, P.xy_blocks, ws.dscal + 0,
-                                           ws.dscal + 1, sdev);
+                                                       ws.dscal + 1, sdev);
       CL_CHECK(cudaGetLastError());
     }
   }

@@ -125,6 +125,8 @@ Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
                                                 const MidRLRatio&, float2*);        \
   extern template Status xy_inv_fwd<EpiJVC>(Context&, const PlanEntry&,             \
                                             const EpiJVC&, float2*);                \
+  extern template Status xy_inv_fwd<EpiRLProduct>(Context&, const PlanEntry&,       \
+                                                  const EpiRLProduct&, float2*);    \
   extern template Status z_pass<ModOTF>(Context&, const PlanEntry&, const ModOTF&,  \
                                         const float2*, float2*);                    \
   extern template Status z_pass<ModWiener>(Context&, const PlanEntry&,              \

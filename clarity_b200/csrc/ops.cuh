@@ -269,14 +269,18 @@ struct EpiJVC {
 // src/ModulateGPU.cu:63-72 / Convolve.cxx:195-205: out = scale * (a * b),
 // no conjugate, a = data, b = OTF; the arithmetic order of
 // ComplexMultiplyAndScale (include/internal/Complex.h:95-102) is kept.
+// scale2 (optional, device memory) multiplies the 1/N scale: the RL flux
+// rescale of the transformed estimate is applied here when the estimate was
+// transformed before its scale was known.
 struct ModOTF {
   static constexpr bool forward_only = false;
   const float2* __restrict__ H;
   float scale;
+  const float* __restrict__ scale2 = nullptr;
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
     const float2 h = __ldg(&H[idx]);
-    return make_float2(scale * (v.x * h.x - v.y * h.y),
-                       scale * (v.x * h.y + v.y * h.x));
+    const float f = scale2 ? scale * *scale2 : scale;
+    return make_float2(f * (v.x * h.x - v.y * h.y), f * (v.x * h.y + v.y * h.x));
   }
 };
 
