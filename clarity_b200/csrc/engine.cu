@@ -501,7 +501,11 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     const float* sk = (k == 0 || !rescale) ? nullptr : sdev;
     CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n, sk}, ws.S, ws.S));
     CL_TRY(xy_inv_fwd(ctx, pe, MidRLRatio{g, P.xmode}, ws.S));
-    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n}, ws.S, ws.S));
+    // the ratio is zero in planes z >= Z (the image is zero there): P3 does
+    // not write them and this pass reads them as zeros
+    ModOTF m4{ws.H, scale_n};
+    m4.zn = id.z;
+    CL_TRY(z_pass(ctx, pe, m4, ws.S, ws.S));
     EpiRLProduct epi;
     epi.cur = (k == 0) ? nullptr : ws.u;
     epi.g = g;

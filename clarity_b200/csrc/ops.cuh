@@ -150,6 +150,9 @@ struct EpiWork {
       out[w.idx(m, y, z)] = c.x;
     return c;
   }
+    // padding rows / z planes where the result is known to be zero
+  __device__ __forceinline__ bool zero_row(int, int) const { return false; }
+  __device__ __forceinline__ bool zero_plane(int) const { return false; }
   __device__ __forceinline__ void finish() {}
 };
 
@@ -175,6 +178,9 @@ struct EpiClip {
     }
     return c;
   }
+    // padding rows / z planes where the result is known to be zero
+  __device__ __forceinline__ bool zero_row(int, int) const { return false; }
+  __device__ __forceinline__ bool zero_plane(int) const { return false; }
   __device__ __forceinline__ void finish() {}
 };
 
@@ -211,6 +217,9 @@ struct EpiRLProduct {
     acc += (double)a;
     return make_float2(a, 0.f);
   }
+    // padding rows / z planes where the result is known to be zero
+  __device__ __forceinline__ bool zero_row(int, int) const { return false; }
+  __device__ __forceinline__ bool zero_plane(int) const { return false; }
   __device__ __forceinline__ void finish() { block_sum_store(acc, partial); }
 };
 
@@ -225,6 +234,11 @@ struct MidRLRatio {
                          rl_ratio(g.at(2 * m + 1, y, z), b.y));
     return make_float2(rl_ratio(g.at(m, y, z), b.x), 0.f);
   }
+    // g is zero outside the image, so the ratio is exactly zero there
+  // (0/b, or the 1e-5 guard): rows with y >= Y and planes with z >= Z need no
+  // transform at all
+  __device__ __forceinline__ bool zero_row(int y, int z) const { return y >= g.Y || z >= g.Z; }
+  __device__ __forceinline__ bool zero_plane(int z) const { return z >= g.Z; }
   __device__ __forceinline__ void finish() {}
 };
 
@@ -262,6 +276,9 @@ struct EpiJVC {
     inext[w.idx(m, y, z)] = r;
     return make_float2(r, 0.f);
   }
+    // padding rows / z planes where the result is known to be zero
+  __device__ __forceinline__ bool zero_row(int, int) const { return false; }
+  __device__ __forceinline__ bool zero_plane(int) const { return false; }
   __device__ __forceinline__ void finish() {}
 };
 
@@ -277,6 +294,9 @@ struct ModOTF {
   const float2* __restrict__ H;
   float scale;
   const float* __restrict__ scale2 = nullptr;
+  // only the first zn z planes of the input spectrum are nonzero (the rest
+  // were never written and are read as zeros)
+  int zn = 1 << 30;
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
     const float2 h = __ldg(&H[idx]);
     const float f = scale2 ? scale * *scale2 : scale;
@@ -290,6 +310,7 @@ struct ModWiener {
   static constexpr bool forward_only = false;
   const float2* __restrict__ H;
   float eps, scale;
+  int zn = 1 << 30;
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
     const float2 h = __ldg(&H[idx]);
     const float mag = h.x * h.x + h.y * h.y;
@@ -301,6 +322,7 @@ struct ModWiener {
 
 struct ModForward {
   static constexpr bool forward_only = true;
+  int zn = 1 << 30;
   __device__ __forceinline__ float2 apply(long long, float2 v) const { return v; }
 };
 

@@ -528,6 +528,9 @@ __global__ void __launch_bounds__(256, 2)
   const int z = blockIdx.x / ngroups;
   const int y0base = (blockIdx.x - z * ngroups) * P.G;
   const float2* twx = tw + P.ax.tw_off;
+  // a plane whose result is known to be zero is neither read nor written;
+  // the next Z pass reads those planes as zeros (Mod::zn)
+  if (mid.zero_plane(z)) return;
   cols_rt<false>(sm, P, S, z, y0base, tw, xrev);
   __syncthreads();
   smem_inverse<true>(sm, P, P.ax, 1, P.G * P.Ay, P.G * P.Ay, P.rowStride, 0, 1, false, twx);
@@ -551,13 +554,17 @@ __global__ void __launch_bounds__(256, 2)
   const long long base = (long long)blockIdx.x * tile;
   // load (16-byte vectors when the tile size is even, which keeps every
   // tile base 16-byte aligned)
-  if ((tile & 1) == 0) {
+  // planes z >= zn of the input are zero (not read)
+  const long long live = (long long)(mod.zn < P.nz ? mod.zn : P.nz) * P.By * P.W;
+  if ((tile & 1) == 0 && (live & 1) == 0) {
     const float4* src = reinterpret_cast<const float4*>(Sin + base);
     float4* dst = reinterpret_cast<float4*>(sm);
-    const int n4 = (int)(tile / 2);
-    for (int t = threadIdx.x; t < n4; t += blockDim.x) dst[t] = __ldg(&src[t]);
+    const int n4 = (int)(tile / 2), live4 = (int)(live / 2);
+    for (int t = threadIdx.x; t < n4; t += blockDim.x)
+      dst[t] = t < live4 ? __ldg(&src[t]) : make_float4(0.f, 0.f, 0.f, 0.f);
   } else {
-    for (int t = threadIdx.x; t < tile; t += blockDim.x) sm[t] = Sin[base + t];
+    for (int t = threadIdx.x; t < tile; t += blockDim.x)
+      sm[t] = t < live ? Sin[base + t] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   const int BW = P.By * P.W;

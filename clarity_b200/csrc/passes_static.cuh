@@ -90,14 +90,30 @@ constexpr unsigned kK1Stride = (unsigned)SH::KG * SH::NZ * SH::BY * SH::W;
 
 // ------------------------------------------------------------------ x rows
 // One register pass S of the x axis over all rows of the XY tile.
-template <class SH, int S, int DIR>
-__device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw) {
+// Row predicates: rows whose content is known to be zero are not transformed.
+struct NoSkip {
+  __device__ __forceinline__ bool operator()(int) const { return false; }
+};
+template <class SH, class F>
+struct RowSkip {
+  const F& f;
+  int z, y0base;
+  __device__ __forceinline__ bool operator()(int r) const {
+    const int g = r / SH::AY, j = r - g * SH::AY;
+    return f.zero_row(y0base + g + SH::BY * j, z);
+  }
+};
+
+template <class SH, int S, int DIR, class Skip>
+__device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw,
+                                       const Skip& skip) {
   using X = typename SH::X;
   constexpr int R = X::radix(S), len = X::len(S), span = len / R;
   constexpr int per_row = X::n / R, total = SH::ROWS * per_row, twstep = X::n / len;
 #pragma unroll 1
   for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
     const int r = f / per_row;
+    if (skip(r)) continue;
     const int rem = f - r * per_row;
     const int b = rem / span;
     const int i = rem - b * span;
@@ -124,21 +140,23 @@ __device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw
   }
 }
 
-template <class SH, int S>
-__device__ __forceinline__ void x_forward_from(float2* sm, const float2* tw) {
+template <class SH, int S, class Skip = NoSkip>
+__device__ __forceinline__ void x_forward_from(float2* sm, const float2* tw,
+                                               const Skip& skip = Skip{}) {
   if constexpr (S < SH::X::npass) {
-    x_pass<SH, S, -1>(sm, tw);
+    x_pass<SH, S, -1>(sm, tw, skip);
     __syncthreads();
-    x_forward_from<SH, S + 1>(sm, tw);
+    x_forward_from<SH, S + 1>(sm, tw, skip);
   }
 }
 
-template <class SH, int S>
-__device__ __forceinline__ void x_inverse_down_to(float2* sm, const float2* tw) {
+template <class SH, int S, class Skip = NoSkip>
+__device__ __forceinline__ void x_inverse_down_to(float2* sm, const float2* tw,
+                                                  const Skip& skip = Skip{}) {
   // inverse passes npass-1 .. S (inclusive)
   if constexpr (S < SH::X::npass) {
-    x_inverse_down_to<SH, S + 1>(sm, tw);
-    x_pass<SH, S, +1>(sm, tw);
+    x_inverse_down_to<SH, S + 1>(sm, tw, skip);
+    x_pass<SH, S, +1>(sm, tw, skip);
     __syncthreads();
   }
 }
@@ -171,9 +189,10 @@ __device__ __forceinline__ void x_first(float2* sm, const Pro& pro, int z, int y
 
 // Last inverse x pass (pass 0) into the epilogue; FUSE re-applies forward
 // pass 0 to what the epilogue returns.
-template <class SH, class Epi, bool FUSE>
+template <class SH, class Epi, bool FUSE, class Skip = NoSkip>
 __device__ __forceinline__ void x_last(float2* sm, Epi& epi, int z, int y0base,
-                                       const float2* __restrict__ tw) {
+                                       const float2* __restrict__ tw,
+                                       const Skip& skip = Skip{}) {
   using X = typename SH::X;
   constexpr int R = X::radix(0), span = X::span(0), total = SH::ROWS * span;
 #pragma unroll 1
@@ -183,6 +202,13 @@ __device__ __forceinline__ void x_last(float2* sm, Epi& epi, int z, int y0base,
     const int g = r / SH::AY, j = r - g * SH::AY;
     const int y = y0base + g + SH::BY * j;
     float2* row = sm + r * SH::ROWSTRIDE;
+    if (skip(r)) {  // known-zero row: its forward transform is zero
+      if constexpr (FUSE) {
+#pragma unroll
+        for (int t = 0; t < R; ++t) row[xp<SH>(i + t * span)] = make_float2(0.f, 0.f);
+      }
+      continue;
+    }
     float2 v[R];
 #pragma unroll
     for (int t = 0; t < R; ++t) v[t] = row[xp<SH>(i + t * span)];
@@ -480,12 +506,16 @@ __global__ void __launch_bounds__(256, 2)
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
   const int y0base = (blockIdx.x - z * SH::NGROUPS) * SH::G;
+  // a plane whose result is known to be zero is neither read nor written;
+  // the next Z pass reads those planes as zeros (Mod::zn)
+  if (mid.zero_plane(z)) return;
+  const RowSkip<SH, Mid> skip{mid, z, y0base};
   cols_inverse<SH>(sm, S, z, y0base, T.twr, T.twny);
   __syncthreads();
-  x_inverse_down_to<SH, 1>(sm, T.twx);
-  x_last<SH, Mid, true>(sm, mid, z, y0base, T.twx);
+  x_inverse_down_to<SH, 1>(sm, T.twx, skip);
+  x_last<SH, Mid, true>(sm, mid, z, y0base, T.twx, skip);
   __syncthreads();
-  x_forward_from<SH, 1>(sm, T.twx);
+  x_forward_from<SH, 1>(sm, T.twx, skip);
   cols_forward<SH>(sm, S, z, y0base, T.twr, T.twny);
   mid.finish();
 }
@@ -499,10 +529,15 @@ __global__ void __launch_bounds__(256, 2)
   const long long base = (long long)blockIdx.x * tile;
   static_assert(tile % 2 == 0, "tile must be even");
   {
+    // planes z >= zn are zero; BW is even so a float4 never spans two planes
+    static_assert(SH::BW % 2 == 0, "tile rows must hold whole float4s");
+    const int zn = mod.zn < SH::NZ ? mod.zn : SH::NZ;
+    const int live4 = zn * SH::BW / 2;
     const float4* src = reinterpret_cast<const float4*>(Sin + base);
     float4* dst = reinterpret_cast<float4*>(sm);
 #pragma unroll 4
-    for (int t = threadIdx.x; t < tile / 2; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) dst[t] = __ldg(&src[t]);
+    for (int t = threadIdx.x; t < tile / 2; t += CLARITY_BLOCK_STRIDE(SH::THREADS))
+      dst[t] = t < live4 ? __ldg(&src[t]) : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
   tile_forward_from<SH, typename SH::Y, 0, false>(sm, T.twy);
@@ -623,6 +658,7 @@ __global__ void __launch_bounds__(256, 2)
   constexpr bool BULK = (BW * 8) % 16 == 0 && (ZS * 8) % 16 == 0;
   using A = typename SH::Z;
   const unsigned gbase = blockIdx.x * (unsigned)SH::TILE;
+  const int zn = mod.zn < NZ ? mod.zn : NZ;  // planes z >= zn are zero
   __shared__ alignas(8) uint64_t bar;
   if constexpr (BULK) {
     static_assert((BW * 8) % 16 == 0 && (ZS * 8) % 16 == 0 && (SH::TILE * 8) % 16 == 0,
@@ -634,9 +670,9 @@ __global__ void __launch_bounds__(256, 2)
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if ((int)threadIdx.x < CLARITY_ISSUE_LANES) {
-      if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, (uint32_t)(NZ * BW * 8));
+      if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, (uint32_t)(zn * BW * 8));
       __syncwarp();
-      for (int z = threadIdx.x; z < NZ; z += CLARITY_ISSUE_LANES)
+      for (int z = threadIdx.x; z < zn; z += CLARITY_ISSUE_LANES)
         bulk_load(sm + z * ZS, Sin + gbase + z * BW, BW * 8, &bar);
     }
     if (!mbar_wait(&bar, 0, T.err)) {
@@ -650,7 +686,10 @@ __global__ void __launch_bounds__(256, 2)
     const int ki = l % W, z = l / W;
     float2 v[BY];
     float2* d = sm + z * ZS + ki;
-    if constexpr (BULK) {
+    if (z >= zn) {
+#pragma unroll
+      for (int y = 0; y < BY; ++y) v[y] = make_float2(0.f, 0.f);
+    } else if constexpr (BULK) {
 #pragma unroll
       for (int y = 0; y < BY; ++y) v[y] = d[y * W];
     } else {
