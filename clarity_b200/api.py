@@ -22,7 +22,9 @@ import threading
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libclarity.so")
+# CLARITY_LIB selects another build of the library (e.g. a variant built
+# with `python -m clarity_b200.build -D... --lib PATH`).
+LIB_PATH = os.environ.get("CLARITY_LIB", os.path.join(_HERE, "libclarity.so"))
 
 # ClarityResult_t (Clarity.h.in:90-101); the numeric order is ABI.
 CLARITY_FFT_FAILED = 0

@@ -56,18 +56,22 @@ def _compile(src: str, obj: str, extra: list[str]) -> tuple[str, int, str]:
 
 
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
-          ptxas_info: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
+          ptxas_info: bool = False, defines: list[str] | None = None,
+          lib: str = LIB, obj_dir: str = OBJ) -> str:
+    """Compile and link.  `defines` adds -D flags (build variants); a variant
+    should use its own `lib` and `obj_dir`."""
+    os.makedirs(obj_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     newest = max((os.path.getmtime(h) for h in _headers()), default=0.0)
     todo = []
     objs = []
     for s in srcs:
-        o = os.path.join(OBJ, os.path.basename(s) + ".o")
+        o = os.path.join(obj_dir, os.path.basename(s) + ".o")
         objs.append(o)
         if force or _stale(s, o, newest):
             todo.append((s, o))
     extra = ["-Xptxas", "-v"] if ptxas_info else []
+    extra += [f"-D{d}" for d in (defines or [])]
     if todo:
         jobs = jobs or min(len(todo), os.cpu_count() or 4)
         with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -81,13 +85,13 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
                     failed.append(src)
             if failed:
                 raise RuntimeError("nvcc failed for: " + ", ".join(failed))
-    if todo or not os.path.exists(LIB):
+    if todo or not os.path.exists(lib):
         cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-cudart", "static",
-               "-o", LIB, *objs]
+               "-o", lib, *objs]
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n" + p.stdout + p.stderr)
-    return LIB
+    return lib
 
 
 def main() -> None:
@@ -96,8 +100,12 @@ def main() -> None:
     ap.add_argument("--jobs", type=int, default=None)
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true")
+    ap.add_argument("-D", dest="defines", action="append", default=[],
+                    help="extra preprocessor definition (build variant)")
+    ap.add_argument("--lib", default=LIB, help="output library path")
+    ap.add_argument("--obj-dir", default=OBJ, help="object directory")
     a = ap.parse_args()
-    print(build(a.force, a.jobs, a.verbose, a.ptxas_info))
+    print(build(a.force, a.jobs, a.verbose, a.ptxas_info, a.defines, a.lib, a.obj_dir))
 
 
 if __name__ == "__main__":

@@ -12,6 +12,12 @@
 #include "plan.hpp"
 #include "tma.cuh"
 
+// Blocks per SM the XY kernels' register budget is sized for (a build
+// option: -DCLARITY_XY_MINBLOCKS=3 trades a few spills for occupancy).
+#ifndef CLARITY_XY_MINBLOCKS
+#define CLARITY_XY_MINBLOCKS 2
+#endif
+
 namespace clarity {
 namespace st {
 
@@ -45,11 +51,14 @@ struct Shape {
   static constexpr int ROWSTRIDE_RAW = (M - 1) + ((M - 1) >> PADSHIFT) + 1;
   static constexpr int ROWSTRIDE = (ROWSTRIDE_RAW % 2 == 0) ? ROWSTRIDE_RAW + 1 : ROWSTRIDE_RAW;
   static constexpr int ROWS = G * AY;
+  // Row groups g are GSTRIDE apart: AY*ROWSTRIDE plus 8 float2 when that is
+  // a multiple of 16, so the column step's groups use disjoint banks.
+  static constexpr int GSTRIDE = AY * ROWSTRIDE + (((AY * ROWSTRIDE) % 16 == 0) ? 8 : 0);
   static constexpr int ITEMS = (M % 2 == 0) ? (M / 2 > 1 ? M / 2 : 1) : (M + 1) / 2;
   static constexpr int BW = BY * W;
   static constexpr int TILE = NZ * BW;
   static constexpr int THREADS = 256;
-  static constexpr int XY_SMEM = ROWS * ROWSTRIDE * 8;
+  static constexpr int XY_SMEM = G * GSTRIDE * 8;
   static constexpr int Z_SMEM = TILE * 8;
   static constexpr int NGROUPS = BY / G;
   // Z kernel with one register pass per y0 line (BY <= 32): padded z stride
@@ -63,6 +72,13 @@ struct Shape {
 template <class SH>
 __device__ __forceinline__ int xp(int e) {
   return e + (e >> SH::PADSHIFT);
+}
+
+// Shared-memory offset of tile row r = g*AY + j.
+template <class SH>
+__device__ __forceinline__ int row_off(int r) {
+  const int g = r / SH::AY, j = r - g * SH::AY;
+  return g * SH::GSTRIDE + j * SH::ROWSTRIDE;
 }
 
 // Digit-reversed slot of natural x frequency k after the DIF passes.
@@ -117,7 +133,7 @@ __device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw
     const int rem = f - r * per_row;
     const int b = rem / span;
     const int i = rem - b * span;
-    float2* row = sm + r * SH::ROWSTRIDE;
+    float2* row = sm + row_off<SH>(r);
     const int e0 = b * len + i;
     float2 v[R];
 #pragma unroll
@@ -181,7 +197,7 @@ __device__ __forceinline__ void x_first(float2* sm, const Pro& pro, int z, int y
 #pragma unroll
       for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k]));
     }
-    float2* row = sm + r * SH::ROWSTRIDE;
+    float2* row = sm + row_off<SH>(r);
 #pragma unroll
     for (int t = 0; t < R; ++t) row[xp<SH>(i + t * span)] = v[t];
   }
@@ -201,7 +217,7 @@ __device__ __forceinline__ void x_last(float2* sm, Epi& epi, int z, int y0base,
     const int i = f - r * span;
     const int g = r / SH::AY, j = r - g * SH::AY;
     const int y = y0base + g + SH::BY * j;
-    float2* row = sm + r * SH::ROWSTRIDE;
+    float2* row = sm + row_off<SH>(r);
     if (skip(r)) {  // known-zero row: its forward transform is zero
       if constexpr (FUSE) {
 #pragma unroll
@@ -268,7 +284,7 @@ __device__ __forceinline__ void cols_forward(const float2* sm, float2* __restric
     const int g = f % SH::G;
     const int it = f / SH::G;
     const int y0 = y0base + g;
-    const float2* rows = sm + (g * AY) * RS;
+    const float2* rows = sm + g * SH::GSTRIDE;
     if (it == 0) {
       const int p0 = xp<SH>(0);
 #pragma unroll 1
@@ -323,7 +339,7 @@ __device__ __forceinline__ void cols_inverse(float2* sm, const float2* __restric
     const int g = f % SH::G;
     const int it = f / SH::G;
     const int y0 = y0base + g;
-    float2* rows = sm + (g * AY) * RS;
+    float2* rows = sm + g * SH::GSTRIDE;
     if (it == 0) {
       const int p0 = xp<SH>(0);
       {
@@ -475,7 +491,7 @@ struct Tables {
 
 // ----------------------------------------------------------------- kernels
 template <class SH, class Pro>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
     ks_xy_forward(const Pro pro, float2* __restrict__ S, const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
@@ -488,7 +504,7 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <class SH, class Epi>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
     ks_xy_inverse(Epi epi, const float2* __restrict__ S, const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
@@ -501,7 +517,7 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <class SH, class Mid>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
     ks_xy_inv_fwd(Mid mid, float2* __restrict__ S, const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
