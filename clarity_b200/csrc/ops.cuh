@@ -12,6 +12,7 @@
 
 #include "dft_codelets.cuh"
 #include "plan.hpp"
+#include "tma.cuh"
 
 namespace clarity {
 
@@ -140,6 +141,7 @@ __device__ __forceinline__ void block_sum_store(double acc, double* partial) {
 
 // Store the real-space result on the work box.
 struct EpiWork {
+  static constexpr bool has_zero_rows = false;
   float* __restrict__ out;
   WorkVol w;
   int xmode;
@@ -153,12 +155,16 @@ struct EpiWork {
     // padding rows / z planes where the result is known to be zero
   __device__ __forceinline__ bool zero_row(int, int) const { return false; }
   __device__ __forceinline__ bool zero_plane(int) const { return false; }
+  // rows y0base + BY*j, j < live_rows, can be nonzero (all here)
+  __device__ __forceinline__ int live_rows(int, int, int ay) const { return ay; }
+  __device__ __forceinline__ void prefetch_row(int, int) const {}
   __device__ __forceinline__ void finish() {}
 };
 
 // Store only the image region (crop from the origin, src/ImageClip.cxx:41-46)
 // into an unpadded (X, Y, Z) volume, times an optional device scale.
 struct EpiClip {
+  static constexpr bool has_zero_rows = false;
   float* __restrict__ out;
   int X, Y, Z;
   const float* __restrict__ scale;
@@ -181,6 +187,9 @@ struct EpiClip {
     // padding rows / z planes where the result is known to be zero
   __device__ __forceinline__ bool zero_row(int, int) const { return false; }
   __device__ __forceinline__ bool zero_plane(int) const { return false; }
+  // rows y0base + BY*j, j < live_rows, can be nonzero (all here)
+  __device__ __forceinline__ int live_rows(int, int, int ay) const { return ay; }
+  __device__ __forceinline__ void prefetch_row(int, int) const {}
   __device__ __forceinline__ void finish() {}
 };
 
@@ -188,6 +197,7 @@ struct EpiClip {
 // step 5 (:73-74): u_new = cur * c, cur = scale * u (or the padded image on
 // the first iteration), partial sums of u_new in FP64.
 struct EpiRLProduct {
+  static constexpr bool has_zero_rows = false;
   const float* __restrict__ cur;     // work-box estimate, or nullptr
   ImageSrc g;                        // used when cur == nullptr
   const float* __restrict__ scale;   // deferred flux scale for cur
@@ -220,12 +230,19 @@ struct EpiRLProduct {
     // padding rows / z planes where the result is known to be zero
   __device__ __forceinline__ bool zero_row(int, int) const { return false; }
   __device__ __forceinline__ bool zero_plane(int) const { return false; }
+  // rows y0base + BY*j, j < live_rows, can be nonzero (all here)
+  __device__ __forceinline__ int live_rows(int, int, int ay) const { return ay; }
+  // the estimate row this block's epilogue will read, into L2
+  __device__ __forceinline__ void prefetch_row(int y, int z) const {
+    if (cur) prefetch_l2_range(cur + w.idx(0, y, z), sizeof(float) * (size_t)w.nx);
+  }
   __device__ __forceinline__ void finish() { block_sum_store(acc, partial); }
 };
 
 // RL step 2 (src/MaximumLikelihoodDeconvolve.cxx:61-62): r = g / (h*u) with
 // the 1e-5 guard, fused between the inverse and forward transforms.
 struct MidRLRatio {
+  static constexpr bool has_zero_rows = true;
   ImageSrc g;
   int xmode;
   __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 b) {
@@ -239,6 +256,15 @@ struct MidRLRatio {
   // transform at all
   __device__ __forceinline__ bool zero_row(int y, int z) const { return y >= g.Y || z >= g.Z; }
   __device__ __forceinline__ bool zero_plane(int z) const { return z >= g.Z; }
+  // rows y0base + by*j with j < live_rows lie inside the image (y < Y)
+  __device__ __forceinline__ int live_rows(int y0base, int by, int ay) const {
+    const int l = (g.Y - y0base + by - 1) / by;
+    return l < 0 ? 0 : (l > ay ? ay : l);
+  }
+  __device__ __forceinline__ void prefetch_row(int y, int z) const {
+    if (y < g.Y && z < g.Z)
+      prefetch_l2_range(g.src + ((unsigned)z * g.Y + y) * g.X, sizeof(float) * (size_t)g.X);
+  }
   __device__ __forceinline__ void finish() {}
 };
 
@@ -248,6 +274,7 @@ struct MidRLRatio {
 // image (first update).  Stores i' on the work box and returns it, so the
 // fused kernel transforms it for the next iteration.
 struct EpiJVC {
+  static constexpr bool has_zero_rows = false;
   const float* __restrict__ cur;
   ImageSrc g;
   float* __restrict__ inext;
@@ -279,6 +306,13 @@ struct EpiJVC {
     // padding rows / z planes where the result is known to be zero
   __device__ __forceinline__ bool zero_row(int, int) const { return false; }
   __device__ __forceinline__ bool zero_plane(int) const { return false; }
+  // rows y0base + BY*j, j < live_rows, can be nonzero (all here)
+  __device__ __forceinline__ int live_rows(int, int, int ay) const { return ay; }
+  __device__ __forceinline__ void prefetch_row(int y, int z) const {
+    if (cur) prefetch_l2_range(cur + w.idx(0, y, z), sizeof(float) * (size_t)w.nx);
+    if (y < g.Y && z < g.Z)
+      prefetch_l2_range(g.src + ((unsigned)z * g.Y + y) * g.X, sizeof(float) * (size_t)g.X);
+  }
   __device__ __forceinline__ void finish() {}
 };
 
@@ -297,6 +331,14 @@ struct ModOTF {
   // only the first zn z planes of the input spectrum are nonzero (the rest
   // were never written and are read as zeros)
   int zn = 1 << 30;
+  // the OTF tile this block will multiply by, into L2 (part p of np)
+  __device__ __forceinline__ void prefetch_tile(unsigned base, int tile, int p, int np) const {
+    const size_t chunk = ((size_t)tile * 8 / np + 15) & ~size_t(15);
+    const size_t off = chunk * p, total = (size_t)tile * 8;
+    if (off < total)
+      prefetch_l2_range(reinterpret_cast<const char*>(H + base) + off,
+                        off + chunk <= total ? chunk : total - off);
+  }
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
     const float2 h = __ldg(&H[idx]);
     const float f = scale2 ? scale * *scale2 : scale;
@@ -311,6 +353,13 @@ struct ModWiener {
   const float2* __restrict__ H;
   float eps, scale;
   int zn = 1 << 30;
+  __device__ __forceinline__ void prefetch_tile(unsigned base, int tile, int p, int np) const {
+    const size_t chunk = ((size_t)tile * 8 / np + 15) & ~size_t(15);
+    const size_t off = chunk * p, total = (size_t)tile * 8;
+    if (off < total)
+      prefetch_l2_range(reinterpret_cast<const char*>(H + base) + off,
+                        off + chunk <= total ? chunk : total - off);
+  }
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
     const float2 h = __ldg(&H[idx]);
     const float mag = h.x * h.x + h.y * h.y;
@@ -323,6 +372,7 @@ struct ModWiener {
 struct ModForward {
   static constexpr bool forward_only = true;
   int zn = 1 << 30;
+  __device__ __forceinline__ void prefetch_tile(unsigned, int, int, int) const {}
   __device__ __forceinline__ float2 apply(long long, float2 v) const { return v; }
 };
 

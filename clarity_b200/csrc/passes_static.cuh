@@ -120,17 +120,33 @@ struct RowSkip {
   }
 };
 
-template <class SH, int S, int DIR, class Skip>
+// Tile rows visited by a pass: all G*AY rows, or (COMPACT) only the first
+// L rows j < L of each group, so threads are not left idle on rows whose
+// content is known to be zero.
+template <class SH, bool COMPACT>
+__device__ __forceinline__ int visit_rows(int L) {
+  return COMPACT ? SH::G * L : SH::ROWS;
+}
+template <class SH, bool COMPACT>
+__device__ __forceinline__ int visit_row(int rv, int L) {
+  if constexpr (!COMPACT) return rv;
+  const int g = rv / L;
+  return g * SH::AY + (rv - g * L);
+}
+
+template <class SH, int S, int DIR, class Skip, bool COMPACT = false>
 __device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw,
-                                       const Skip& skip) {
+                                       const Skip& skip, int L = SH::AY) {
   using X = typename SH::X;
   constexpr int R = X::radix(S), len = X::len(S), span = len / R;
-  constexpr int per_row = X::n / R, total = SH::ROWS * per_row, twstep = X::n / len;
+  constexpr int per_row = X::n / R, twstep = X::n / len;
+  const int total = visit_rows<SH, COMPACT>(L) * per_row;
 #pragma unroll 1
   for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
-    const int r = f / per_row;
+    const int rv = f / per_row;
+    const int r = visit_row<SH, COMPACT>(rv, L);
     if (skip(r)) continue;
-    const int rem = f - r * per_row;
+    const int rem = f - rv * per_row;
     const int b = rem / span;
     const int i = rem - b * span;
     float2* row = sm + row_off<SH>(r);
@@ -156,23 +172,23 @@ __device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw
   }
 }
 
-template <class SH, int S, class Skip = NoSkip>
+template <class SH, int S, class Skip = NoSkip, bool COMPACT = false>
 __device__ __forceinline__ void x_forward_from(float2* sm, const float2* tw,
-                                               const Skip& skip = Skip{}) {
+                                               const Skip& skip = Skip{}, int L = SH::AY) {
   if constexpr (S < SH::X::npass) {
-    x_pass<SH, S, -1>(sm, tw, skip);
+    x_pass<SH, S, -1, Skip, COMPACT>(sm, tw, skip, L);
     __syncthreads();
-    x_forward_from<SH, S + 1>(sm, tw, skip);
+    x_forward_from<SH, S + 1, Skip, COMPACT>(sm, tw, skip, L);
   }
 }
 
-template <class SH, int S, class Skip = NoSkip>
+template <class SH, int S, class Skip = NoSkip, bool COMPACT = false>
 __device__ __forceinline__ void x_inverse_down_to(float2* sm, const float2* tw,
-                                                  const Skip& skip = Skip{}) {
+                                                  const Skip& skip = Skip{}, int L = SH::AY) {
   // inverse passes npass-1 .. S (inclusive)
   if constexpr (S < SH::X::npass) {
-    x_inverse_down_to<SH, S + 1>(sm, tw, skip);
-    x_pass<SH, S, +1>(sm, tw, skip);
+    x_inverse_down_to<SH, S + 1, Skip, COMPACT>(sm, tw, skip, L);
+    x_pass<SH, S, +1, Skip, COMPACT>(sm, tw, skip, L);
     __syncthreads();
   }
 }
@@ -205,16 +221,18 @@ __device__ __forceinline__ void x_first(float2* sm, const Pro& pro, int z, int y
 
 // Last inverse x pass (pass 0) into the epilogue; FUSE re-applies forward
 // pass 0 to what the epilogue returns.
-template <class SH, class Epi, bool FUSE, class Skip = NoSkip>
+template <class SH, class Epi, bool FUSE, class Skip = NoSkip, bool COMPACT = false>
 __device__ __forceinline__ void x_last(float2* sm, Epi& epi, int z, int y0base,
                                        const float2* __restrict__ tw,
-                                       const Skip& skip = Skip{}) {
+                                       const Skip& skip = Skip{}, int L = SH::AY) {
   using X = typename SH::X;
-  constexpr int R = X::radix(0), span = X::span(0), total = SH::ROWS * span;
+  constexpr int R = X::radix(0), span = X::span(0);
+  const int total = visit_rows<SH, COMPACT>(L) * span;
 #pragma unroll 1
   for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
-    const int r = f / span;
-    const int i = f - r * span;
+    const int rv = f / span;
+    const int r = visit_row<SH, COMPACT>(rv, L);
+    const int i = f - rv * span;
     const int g = r / SH::AY, j = r - g * SH::AY;
     const int y = y0base + g + SH::BY * j;
     float2* row = sm + row_off<SH>(r);
@@ -503,12 +521,24 @@ __global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
   pro.finish();
 }
 
+// Rows the epilogue reads are prefetched into L2 at kernel start, so their
+// loads hit L2 by the time the transforms reach them.
+template <class SH, class Epi>
+__device__ __forceinline__ void prefetch_tile_rows(const Epi& epi, int z, int y0base) {
+  if ((int)threadIdx.x < SH::ROWS) {
+    const int r = threadIdx.x;
+    const int g = r / SH::AY, j = r - g * SH::AY;
+    epi.prefetch_row(y0base + g + SH::BY * j, z);
+  }
+}
+
 template <class SH, class Epi>
 __global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
     ks_xy_inverse(Epi epi, const float2* __restrict__ S, const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
   const int y0base = (blockIdx.x - z * SH::NGROUPS) * SH::G;
+  prefetch_tile_rows<SH>(epi, z, y0base);
   cols_inverse<SH>(sm, S, z, y0base, T.twr, T.twny);
   __syncthreads();
   x_inverse_down_to<SH, 1>(sm, T.twx);
@@ -525,13 +555,29 @@ __global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
   // a plane whose result is known to be zero is neither read nor written;
   // the next Z pass reads those planes as zeros (Mod::zn)
   if (mid.zero_plane(z)) return;
+  prefetch_tile_rows<SH>(mid, z, y0base);
   const RowSkip<SH, Mid> skip{mid, z, y0base};
   cols_inverse<SH>(sm, S, z, y0base, T.twr, T.twny);
   __syncthreads();
-  x_inverse_down_to<SH, 1>(sm, T.twx, skip);
-  x_last<SH, Mid, true>(sm, mid, z, y0base, T.twx, skip);
-  __syncthreads();
-  x_forward_from<SH, 1>(sm, T.twx, skip);
+  if constexpr (Mid::has_zero_rows) {
+    // only rows j < L of each group can be nonzero; the others are zeroed
+    const int L = mid.live_rows(y0base, SH::BY, SH::AY);
+    x_inverse_down_to<SH, 1, RowSkip<SH, Mid>, true>(sm, T.twx, skip, L);
+    x_last<SH, Mid, true, RowSkip<SH, Mid>, true>(sm, mid, z, y0base, T.twx, skip, L);
+    const int dead = SH::G * (SH::AY - L) * SH::ROWSTRIDE;
+    for (int t = threadIdx.x; t < dead; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+      const int rd = t / SH::ROWSTRIDE, e = t - rd * SH::ROWSTRIDE;
+      const int g = rd / (SH::AY - L), j = L + (rd - g * (SH::AY - L));
+      sm[g * SH::GSTRIDE + j * SH::ROWSTRIDE + e] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    x_forward_from<SH, 1, RowSkip<SH, Mid>, true>(sm, T.twx, skip, L);
+  } else {
+    x_inverse_down_to<SH, 1>(sm, T.twx, skip);
+    x_last<SH, Mid, true>(sm, mid, z, y0base, T.twx, skip);
+    __syncthreads();
+    x_forward_from<SH, 1>(sm, T.twx, skip);
+  }
   cols_forward<SH>(sm, S, z, y0base, T.twr, T.twny);
   mid.finish();
 }
@@ -543,6 +589,7 @@ __global__ void __launch_bounds__(256, 2)
   CLARITY_DYN_SMEM(float2, sm);
   constexpr int tile = SH::TILE;
   const long long base = (long long)blockIdx.x * tile;
+  if (threadIdx.x < 16) mod.prefetch_tile((unsigned)base, tile, threadIdx.x, 16);
   static_assert(tile % 2 == 0, "tile must be even");
   {
     // planes z >= zn are zero; BW is even so a float4 never spans two planes
@@ -675,6 +722,7 @@ __global__ void __launch_bounds__(256, 2)
   using A = typename SH::Z;
   const unsigned gbase = blockIdx.x * (unsigned)SH::TILE;
   const int zn = mod.zn < NZ ? mod.zn : NZ;  // planes z >= zn are zero
+  if (threadIdx.x < 16) mod.prefetch_tile(gbase, SH::TILE, threadIdx.x, 16);
   __shared__ alignas(8) uint64_t bar;
   if constexpr (BULK) {
     static_assert((BW * 8) % 16 == 0 && (ZS * 8) % 16 == 0 && (SH::TILE * 8) % 16 == 0,

@@ -8,6 +8,7 @@
 // records an error code in *err and gives up, so a lost completion can
 // never hang the GPU.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 
 #include "launch_macro.cuh"
@@ -70,9 +71,14 @@ __device__ __forceinline__ void fence_smem_to_async() {
 __device__ __forceinline__ bool smem_aligned16(const void* p) {
   return (smem_u32(p) & 15u) == 0;
 }
+// Hint: bring [p, p+bytes) into L2 (p and bytes multiples of 16).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 #else
 // Host emulation: copies happen immediately.
 inline bool smem_aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+inline void prefetch_l2(const void*, uint32_t) {}
 inline void mbar_init(uint64_t* bar, uint32_t) { *bar = 0; }
 inline void mbar_arrive_expect_tx(uint64_t*, uint32_t) {}
 inline bool mbar_try_wait(uint64_t*, uint32_t) { return true; }
@@ -90,6 +96,15 @@ inline int atomicExch(int* p, int v) {
   return o;
 }
 #endif
+
+// L2 prefetch of the 16-byte-aligned part of [begin, begin+bytes): never
+// touches memory outside the range.
+__device__ __forceinline__ void prefetch_l2_range(const void* begin, size_t bytes) {
+  const uintptr_t b = reinterpret_cast<uintptr_t>(begin);
+  const uintptr_t lo = (b + 15) & ~uintptr_t(15);
+  const uintptr_t hi = (b + bytes) & ~uintptr_t(15);
+  if (hi > lo) prefetch_l2(reinterpret_cast<const void*>(lo), (uint32_t)(hi - lo));
+}
 
 // Bounded wait for phase `parity` of the barrier; false (and *err set) on
 // timeout.
