@@ -750,10 +750,12 @@ __global__ void __launch_bounds__(256, 2)
     const int ki = l % W, z = l / W;
     float2 v[BY];
     float2* d = sm + z * ZS + ki;
-    if (z >= zn) {
+    if (z >= zn) {  // known-zero plane: its transform is zero
 #pragma unroll
-      for (int y = 0; y < BY; ++y) v[y] = make_float2(0.f, 0.f);
-    } else if constexpr (BULK) {
+      for (int k = 0; k < BY; ++k) d[k * W] = make_float2(0.f, 0.f);
+      continue;
+    }
+    if constexpr (BULK) {
 #pragma unroll
       for (int y = 0; y < BY; ++y) v[y] = d[y * W];
     } else {
