@@ -180,11 +180,19 @@ def family_bytes(work, img_vox, ker_vox, iters):
     return {
         "xy_forward": (Rk + C) + (Ri + C),
         "z": 2 * C + 2 * iters * 3 * C,
-        "xy_inv_fwd": iters * (2 * C + Ri) + sum(prod_merged),
+        "xy_inv_fwd": iters * (2 * C + Ri),
+        "xy_product": sum(prod_merged),
         "xy_inverse": last,
         "per_iteration": 2 * R + Ri + 10 * C,
         "per_iteration_survey": 4 * R + 10 * C,
     }
+
+
+# DRAM bytes (read + write) per launch of each steady-iteration kernel family,
+# from the ncu capture of iteration 2 of this workload
+# (profiles/kernels_rl_iteration_512x512x128.md; z: mean of its two launches).
+NCU_TRAFFIC = {"xy_product": 278.6e6 + 223.9e6, "xy_inv_fwd": 85.1e6 + 33.1e6,
+               "z": (271.5e6 + 87.8e6 + 203.5e6 + 87.8e6) / 2}
 
 
 def run_gpu_arm(args, rank, world):
@@ -292,7 +300,8 @@ def run_gpu_arm(args, rank, world):
         achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "bytes_per_launch": bytes_per_launch,
+                "traffic": NCU_TRAFFIC.get(dom), "traffic_unit": "bytes per launch",
+                "bytes_per_launch": bytes_per_launch,
                 "ms_per_launch": per_launch_ms,
                 "share_of_step": tot_ms / ms_total}
     iter_bytes = fb["per_iteration_survey"]

@@ -289,7 +289,7 @@ def plan_info(work_shape_zyx) -> dict:
 
 
 # ------------------------------------------------------------ probes
-KERNEL_FAMILIES = ["xy_forward", "z", "xy_inv_fwd", "xy_inverse", "other"]
+KERNEL_FAMILIES = ["xy_forward", "z", "xy_inv_fwd", "xy_inverse", "other", "xy_product"]
 
 
 def launch_count() -> int:
@@ -301,9 +301,10 @@ def timing_enable(on: bool = True) -> None:
 
 
 def timing_collect() -> dict:
-    ms = (C.c_double * 5)()
-    cnt = (C.c_longlong * 5)()
-    load().clarityx_timing_collect(ms, cnt, 5)
+    n = len(KERNEL_FAMILIES)
+    ms = (C.c_double * n)()
+    cnt = (C.c_longlong * n)()
+    load().clarityx_timing_collect(ms, cnt, n)
     return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_FAMILIES)}
 
 

@@ -14,7 +14,11 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
+#ifndef CLARITY_HOST_EMULATION
+#include <cudaTypedefs.h>
+#endif
 #include "engine.hpp"
 #include "launch.cuh"
 #include "ops.cuh"
@@ -100,6 +104,52 @@ int static_family_mask() {
 
 static inline void count_small() { g_launches.fetch_add(1); }
 
+bool xy_tma_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("CLARITY_XY_TMA");
+    return !(v && v[0] == '0');
+  }();
+  return on;
+}
+
+#ifndef CLARITY_HOST_EMULATION
+// cuTensorMapEncodeTiled, fetched from the driver through the runtime (no
+// link-time dependency on libcuda).
+bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
+                          const unsigned long long stride_bytes[3], const unsigned box[4]) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      fn = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }();
+  if (!encode || ((uintptr_t)base & 15u) != 0) return false;
+  const cuuint64_t gdim[4] = {dim[0], dim[1], dim[2], dim[3]};
+  const cuuint64_t gstr[3] = {stride_bytes[0], stride_bytes[1], stride_bytes[2]};
+  const cuuint32_t bdim[4] = {box[0], box[1], box[2], box[3]};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), gdim, gstr,
+                bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+#else
+bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
+                          const unsigned long long stride_bytes[3], const unsigned box[4]) {
+  if (((uintptr_t)base & 15u) != 0) return false;
+  tm->base = static_cast<char*>(const_cast<void*>(base));
+  for (int d = 0; d < 4; ++d) {
+    tm->dim[d] = dim[d];
+    tm->box[d] = box[d];
+    tm->stride[d] = d == 0 ? 4 : stride_bytes[d - 1];
+  }
+  return true;
+}
+#endif
+
 void timing_enable(bool on) { g_timing.store(on); }
 
 void timing_collect(double* ms, long long* counts) {
@@ -166,10 +216,10 @@ __global__ void k_finish_sum(const double* partial, int np, double* dout) {
 // RL flux scale (src/MaximumLikelihoodDeconvolve.cxx:73-78):
 // scale = energy / newEnergy with both rounded to float first, as the
 // reference holds them in floats.
-__global__ void k_finish_rl_scale(const double* partial, int np,
+__global__ void k_finish_rl_scale(const double* partial, const int* np,
                                   const double* energy, double* sum_out,
                                   float* scale_out) {
-  const double t = block_total(partial, np);
+  const double t = block_total(partial, *np);
   if (threadIdx.x == 0) {
     sum_out[0] = t;
     scale_out[0] = (float)energy[0] / (float)t;
@@ -276,7 +326,8 @@ Context::~Context() {
 void Context::release_workspaces() {
   Workspace& w = ws_;
   cudaFree(w.S); cudaFree(w.H); cudaFree(w.u); cudaFree(w.img); cudaFree(w.ker);
-  cudaFree(w.partial); cudaFree(w.dscal); cudaFree(w.fscal);
+  cudaFree(w.partial); cudaFree(w.dscal); cudaFree(w.fscal); cudaFree(w.iscal);
+  cudaFree(w.HG);
   w = Workspace();
 }
 
@@ -353,8 +404,8 @@ Status Context::workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
   long long sc = w.spec_cap;
   Status s;
   if (w.spec_cap < P.spec_elems || !w.S || !w.H) {
-    cudaFree(w.S); cudaFree(w.H);
-    w.S = w.H = nullptr;
+    cudaFree(w.S); cudaFree(w.H); cudaFree(w.HG);
+    w.S = w.H = w.HG = nullptr;
     w.spec_cap = 0;
     CL_CHECK(dev_alloc((void**)&w.S, sizeof(float2) * (size_t)P.spec_elems));
     CL_CHECK(dev_alloc((void**)&w.H, sizeof(float2) * (size_t)P.spec_elems));
@@ -371,11 +422,15 @@ Status Context::workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
   if (!s.ok()) return s;
   w.ker_cap = (size_t)kc;
   long long pc = w.partial_cap;
-  s = ensure(&w.partial, &pc, std::max<long long>(std::max(P.xy_blocks, kReduceBlocks), 1));
+  // one partial per XY block: at most one block per (z, y0) line
+  s = ensure(&w.partial, &pc,
+             std::max<long long>({(long long)P.xy_blocks, (long long)P.nz * P.By,
+                                  (long long)kReduceBlocks, 1}));
   if (!s.ok()) return s;
   w.partial_cap = (int)pc;
   if (!w.dscal) CL_CHECK(dev_alloc((void**)&w.dscal, sizeof(double) * 16));
   if (!w.fscal) CL_CHECK(dev_alloc((void**)&w.fscal, sizeof(float) * 16));
+  if (!w.iscal) CL_CHECK(dev_alloc((void**)&w.iscal, sizeof(int) * 16));
   *out = &w;
   return Status::Ok();
 }
@@ -515,13 +570,14 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     epi.w = wv;
     epi.xmode = P.xmode;
     epi.acc = 0.0;
+    epi.nblocks = ws.iscal;  // the partials' count, as launched
     if (k + 1 < iters)
       CL_TRY(xy_inv_fwd(ctx, pe, epi, ws.S));
     else
       CL_TRY(xy_inverse(ctx, pe, epi, ws.S));
     if (rescale) {
       count_small();
-      CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws.partial, P.xy_blocks, ws.dscal + 0,
+      CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws.partial, ws.iscal, ws.dscal + 0,
                                                        ws.dscal + 1, sdev);
       CL_CHECK(cudaGetLastError());
     }
@@ -583,9 +639,44 @@ Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
 // Jansen-van Cittert: the first update reads the padded image; every update
 // is a z pass (h * i) plus one fused XY pass (inverse, JVC update, store i',
 // forward transform of i' for the next update).
+// Sampled Gaussian smoothing kernel of the work-box size (smoothed JVC):
+// exp(-d^2 / (2 sigma^2)) per axis about the centre n/2, a delta along an
+// axis with sigma <= 0, normalised to unit sum in double and rounded to float.
+// Treated as a PSF (pad/shift by -n/2), its OTF convolves the estimate with a
+// Gaussian centred at the origin.
+static std::vector<float> gauss_kernel(Dims wd, const float* sigma) {
+  const int n[3] = {wd.x, wd.y, wd.z};
+  std::vector<double> ax[3];
+  for (int d = 0; d < 3; ++d) {
+    ax[d].resize(n[d]);
+    const int c = n[d] / 2;
+    const double s = sigma[d];
+    for (int i = 0; i < n[d]; ++i) {
+      const double t = i - c;
+      ax[d][i] = s > 0 ? std::exp(-t * t / (2.0 * s * s)) : (i == c ? 1.0 : 0.0);
+    }
+  }
+  double sum = 0;
+  for (int z = 0; z < n[2]; ++z)
+    for (int y = 0; y < n[1]; ++y)
+      for (int x = 0; x < n[0]; ++x) sum += ax[2][z] * ax[1][y] * ax[0][x];
+  std::vector<float> k((size_t)wd.n());
+  size_t o = 0;
+  for (int z = 0; z < n[2]; ++z)
+    for (int y = 0; y < n[1]; ++y)
+      for (int x = 0; x < n[0]; ++x) k[o++] = (float)(ax[2][z] * ax[1][y] * ax[0][x] / sum);
+  return k;
+}
+
+// JVC (src/JansenVanCittertDeconvolve.cxx:311-389), two fused passes per
+// update.  Smoothed JVC (smooth_interval > 0; the reference body writes
+// zeros, src/SmoothedJansenVanCittertDeconvolve.cxx:27-40): after every
+// smooth_interval-th update the work-box estimate is convolved with
+// gauss_kernel(smooth_sigma) -- one z pass with the kernel's OTF and one xy
+// pass that stores the smoothed estimate (and transforms it on).
 Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
                Dims kd, float* out, int iters, float /*image_max*/,
-               const float* /*smooth_sigma*/, int /*smooth_interval*/) {
+               const float* smooth_sigma, int smooth_interval) {
   const PlanEntry* pe;
   Workspace* ws;
   Dims wd;
@@ -604,18 +695,39 @@ Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
   CL_CHECK(cudaMemcpyAsync(hc, ws->fscal + 4, sizeof(hc), cudaMemcpyDeviceToHost, st));
   CL_CHECK(cudaStreamSynchronize(st));
   CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  const bool smooth = smooth_sigma != nullptr && smooth_interval > 0;
+  if (smooth) {
+    // the smoothing kernel's OTF; ws->u holds the kernel meanwhile (the
+    // estimate is first written by the first update)
+    if (!ws->HG) CL_CHECK(dev_alloc((void**)&ws->HG, sizeof(float2) * (size_t)ws->spec_cap));
+    const std::vector<float> gk = gauss_kernel(wd, smooth_sigma);
+    CL_CHECK(cudaMemcpyAsync(ws->u, gk.data(), sizeof(float) * gk.size(),
+                             cudaMemcpyHostToDevice, st));
+    CL_TRY(make_otf(ctx, *pe, ws->u, wd, wd, ws->HG, nullptr));
+    CL_CHECK(cudaStreamSynchronize(st));  // gk is pageable host memory
+  }
   const ImageSrc g = image_src(img, id);
   const WorkVol wv{wd.x, wd.y, wd.z};
   const float scale_n = inv_volume(wd);
   const int total = iters > 1 ? iters : 1;
   CL_TRY(xy_forward(ctx, *pe, ProImage{g, P.xmode}, ws->S));
   for (int k = 0; k < total; ++k) {
+    const bool last = k + 1 == total;
+    const bool smooth_now = smooth && (k + 1) % smooth_interval == 0;
     CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, scale_n}, ws->S, ws->S));
     EpiJVC epi{k == 0 ? nullptr : ws->u, g, ws->u, hc[0], hc[1], wv, P.xmode};
-    if (k + 1 < total)
+    if (!last || smooth_now)
       CL_TRY(xy_inv_fwd(ctx, *pe, epi, ws->S));
     else
       CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
+    if (smooth_now) {
+      CL_TRY(z_pass(ctx, *pe, ModOTF{ws->HG, scale_n}, ws->S, ws->S));
+      const EpiWork ew{ws->u, wv, P.xmode};
+      if (!last)
+        CL_TRY(xy_inv_fwd(ctx, *pe, ew, ws->S));
+      else
+        CL_TRY(xy_inverse(ctx, *pe, ew, ws->S));
+    }
   }
   count_small();
   CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,

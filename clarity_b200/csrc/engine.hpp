@@ -49,12 +49,14 @@ void set_alloc_failure_countdown(int n);
 struct Workspace {
   float2* S = nullptr;     // work spectrum (S layout)
   float2* H = nullptr;     // OTF (S layout)
+  float2* HG = nullptr;    // smoothing-kernel OTF (S layout; smoothed JVC only)
   float* u = nullptr;      // work-box real volume (estimate)
   float* img = nullptr;    // unpadded image
   float* ker = nullptr;    // unpadded kernel
   double* partial = nullptr;
   double* dscal = nullptr; // [0] energy, [1] last sum, [2..] misc
   float* fscal = nullptr;  // [0] deferred scale, [1] ones, [2..] misc
+  int* iscal = nullptr;    // [0] number of partial sums the last product pass wrote
   size_t img_cap = 0, ker_cap = 0;
   long long spec_cap = 0, work_cap = 0;
   int partial_cap = 0;
@@ -108,9 +110,6 @@ Context* global_context();  // nullptr when not registered
 void set_last_error(const char* msg);
 
 // ------------------------------------------------ launch accounting
-// Kernel families timed by the optional event probes.
-enum KernelKind { KK_XY_FORWARD = 0, KK_Z = 1, KK_XY_INV_FWD = 2, KK_XY_INVERSE = 3,
-                  KK_OTHER = 4, KK_COUNT = 5 };
 // Counts every kernel launch of the library (for benchmarks) and, when
 // timing is enabled, records a CUDA event pair around each fused-pass launch
 // on the launching stream.

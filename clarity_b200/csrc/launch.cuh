@@ -80,10 +80,10 @@ Status xy_inv_fwd(Context& ctx, const PlanEntry& pe, const Mid& mid,
     return status_from_cuda(se, "xy inverse+forward");
   auto k = k_xy_inv_fwd<Mid>;
   CL_CHECK(prep_kernel(k, P.xy_smem));
-  note_launch_begin(KK_XY_INV_FWD, ctx.exec_stream());
+  note_launch_begin(family_of<Mid, KK_XY_INV_FWD>(), ctx.exec_stream());
   CLARITY_LAUNCH(k, P.xy_blocks, P.xy_threads, P.xy_smem, ctx.exec_stream())(P, mid, S, pe.tw,
                                                                  pe.xrev);
-  note_launch_end(KK_XY_INV_FWD, ctx.exec_stream());
+  note_launch_end(family_of<Mid, KK_XY_INV_FWD>(), ctx.exec_stream());
   CL_CHECK(cudaGetLastError());
   return Status::Ok();
 }
@@ -127,6 +127,8 @@ Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
                                             const EpiJVC&, float2*);                \
   extern template Status xy_inv_fwd<EpiRLProduct>(Context&, const PlanEntry&,       \
                                                   const EpiRLProduct&, float2*);    \
+  extern template Status xy_inv_fwd<EpiWork>(Context&, const PlanEntry&,            \
+                                             const EpiWork&, float2*);              \
   extern template Status z_pass<ModOTF>(Context&, const PlanEntry&, const ModOTF&,  \
                                         const float2*, float2*);                    \
   extern template Status z_pass<ModWiener>(Context&, const PlanEntry&,              \

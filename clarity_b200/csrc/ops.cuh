@@ -15,6 +15,14 @@
 #include "tma.cuh"
 
 namespace clarity {
+namespace st {
+// A tile row's input for the staged pass kernels: nf floats at p
+// (x = 0 .. nf-1), zero beyond; nf == 0 for a row known to be zero.
+struct RowRef {
+  const float* p;
+  int nf;
+};
+}  // namespace st
 
 // The reference divide of src/ComputePrimitives.cxx:144-148 (and
 // ComputePrimitivesGPU.cu:180-184) tests fabs(b) < 1e-5 in double; for a
@@ -198,6 +206,7 @@ struct EpiClip {
 // the first iteration), partial sums of u_new in FP64.
 struct EpiRLProduct {
   static constexpr bool has_zero_rows = false;
+  static constexpr int kFamily = KK_XY_PRODUCT;
   const float* __restrict__ cur;     // work-box estimate, or nullptr
   ImageSrc g;                        // used when cur == nullptr
   const float* __restrict__ scale;   // deferred flux scale for cur
@@ -206,6 +215,7 @@ struct EpiRLProduct {
   WorkVol w;
   int xmode;
   double acc;
+  int* nblocks;  // receives the grid size (the number of partials), or nullptr
   __device__ __forceinline__ float cur_at(int x, int y, int z) const {
     if (cur) {
       const float u = __ldg(&cur[w.idx(x, y, z)]);
@@ -236,7 +246,36 @@ struct EpiRLProduct {
   __device__ __forceinline__ void prefetch_row(int y, int z) const {
     if (cur) prefetch_l2_range(cur + w.idx(0, y, z), sizeof(float) * (size_t)w.nx);
   }
-  __device__ __forceinline__ void finish() { block_sum_store(acc, partial); }
+  // Staged form (passes_xy_tma.cuh): row (y, z) of cur (or of the image on
+  // the first iteration) arrives in shared memory; u' overwrites it there and
+  // leaves by a bulk store to unew.
+  static constexpr bool kStaged = true;
+  static constexpr bool kStoreRows = true;
+  __device__ __forceinline__ st::RowRef in_row(int y, int z) const {
+    if (cur) return {cur + w.idx(0, y, z), w.nx};
+    if (y < g.Y && z < g.Z) return {g.src + ((unsigned)z * g.Y + y) * g.X, g.X};
+    return {nullptr, 0};
+  }
+  __device__ __forceinline__ float* out_row(int y, int z) const { return unew + w.idx(0, y, z); }
+  __device__ __forceinline__ float2 apply_s(int m, int, int, float2 c, float* sr, int n) {
+    const int x = 2 * m;
+    float u0 = x < n ? sr[x] : 0.f, u1 = x + 1 < n ? sr[x + 1] : 0.f;
+    if (cur && scale) {
+      const float s = __ldg(scale);
+      u0 = s * u0;
+      u1 = s * u1;
+    }
+    const float a = u0 * c.x, b = u1 * c.y;
+    sr[x] = a;
+    sr[x + 1] = b;
+    acc += (double)a;
+    acc += (double)b;
+    return make_float2(a, b);
+  }
+  __device__ __forceinline__ void finish() {
+    block_sum_store(acc, partial);
+    if (nblocks && blockIdx.x == 0 && threadIdx.x == 0) *nblocks = (int)gridDim.x;
+  }
 };
 
 // RL step 2 (src/MaximumLikelihoodDeconvolve.cxx:61-62): r = g / (h*u) with
@@ -264,6 +303,18 @@ struct MidRLRatio {
   __device__ __forceinline__ void prefetch_row(int y, int z) const {
     if (y < g.Y && z < g.Z)
       prefetch_l2_range(g.src + ((unsigned)z * g.Y + y) * g.X, sizeof(float) * (size_t)g.X);
+  }
+  // Staged form: the image row arrives in shared memory.
+  static constexpr bool kStaged = true;
+  static constexpr bool kStoreRows = false;
+  __device__ __forceinline__ st::RowRef in_row(int y, int z) const {
+    if (y < g.Y && z < g.Z) return {g.src + ((unsigned)z * g.Y + y) * g.X, g.X};
+    return {nullptr, 0};
+  }
+  __device__ __forceinline__ float* out_row(int, int) const { return nullptr; }
+  __device__ __forceinline__ float2 apply_s(int m, int, int, float2 b, float* sr, int n) const {
+    const int x = 2 * m;
+    return make_float2(rl_ratio(x < n ? sr[x] : 0.f, b.x), rl_ratio(x + 1 < n ? sr[x + 1] : 0.f, b.y));
   }
   __device__ __forceinline__ void finish() {}
 };

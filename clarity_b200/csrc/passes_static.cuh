@@ -266,10 +266,12 @@ __device__ __forceinline__ void x_last(float2* sm, Epi& epi, int z, int y0base,
 }
 
 // ------------------------------------------------------- r2c / c2r columns
+// Column kx of the group's rows after the Ay-DFT: twiddled by w_ny^(y0*k1)
+// and stored to S[k1][kx][z][y0] (store_col), or loaded and untwiddled
+// (load_col) before the inverse Ay-DFT.
 template <class SH>
-__device__ __forceinline__ void split_store(float2* v, float2* __restrict__ S, int kx,
-                                            int z, int y0, const float2* __restrict__ twny) {
-  dft<SH::AY, -1>(v);
+__device__ __forceinline__ void store_col(const float2* v, float2* __restrict__ S, int kx,
+                                          int z, int y0, const float2* __restrict__ twny) {
   float2* dst = S + sbase<SH>(kx, z, y0);
 #pragma unroll
   for (int k1 = 0; k1 < SH::AY; ++k1) {
@@ -279,8 +281,8 @@ __device__ __forceinline__ void split_store(float2* v, float2* __restrict__ S, i
 }
 
 template <class SH>
-__device__ __forceinline__ void split_load(float2* v, const float2* __restrict__ S, int kx,
-                                           int z, int y0, const float2* __restrict__ twny) {
+__device__ __forceinline__ void load_col(float2* v, const float2* __restrict__ S, int kx,
+                                         int z, int y0, const float2* __restrict__ twny) {
   const float2* src = S + sbase<SH>(kx, z, y0);
 #pragma unroll
   for (int k1 = 0; k1 < SH::AY; ++k1) {
@@ -288,6 +290,19 @@ __device__ __forceinline__ void split_load(float2* v, const float2* __restrict__
     if (k1 != 0 && y0 != 0) a = cmulc(a, __ldg(&twny[y0 * k1]));
     v[k1] = a;
   }
+}
+
+template <class SH>
+__device__ __forceinline__ void split_store(float2* v, float2* __restrict__ S, int kx,
+                                            int z, int y0, const float2* __restrict__ twny) {
+  dft<SH::AY, -1>(v);
+  store_col<SH>(v, S, kx, z, y0, twny);
+}
+
+template <class SH>
+__device__ __forceinline__ void split_load(float2* v, const float2* __restrict__ S, int kx,
+                                           int z, int y0, const float2* __restrict__ twny) {
+  load_col<SH>(v, S, kx, z, y0, twny);
   dft<SH::AY, +1>(v);
 }
 
@@ -304,16 +319,26 @@ __device__ __forceinline__ void cols_forward(const float2* sm, float2* __restric
     const int y0 = y0base + g;
     const float2* rows = sm + g * SH::GSTRIDE;
     if (it == 0) {
+      // kx = 0 and kx = M have real columns a, b: one DFT of a + i b gives
+      // both, A[k] = (P[k] + conj P[-k]) / 2, B[k] = (P[k] - conj P[-k]) / 2i
       const int p0 = xp<SH>(0);
-#pragma unroll 1
-      for (int side = 0; side < 2; ++side) {
-        float2 xc[AY];
+      {
+        float2 pk[AY];
 #pragma unroll
         for (int j = 0; j < AY; ++j) {
           const float2 Z0 = rows[j * RS + p0];
-          xc[j] = make_float2(side == 0 ? Z0.x + Z0.y : Z0.x - Z0.y, 0.f);
+          pk[j] = make_float2(Z0.x + Z0.y, Z0.x - Z0.y);
         }
-        split_store<SH>(xc, S, side == 0 ? 0 : M, z, y0, twny);
+        dft<AY, -1>(pk);
+        float2 a[AY], b[AY];
+#pragma unroll
+        for (int k = 0; k < AY; ++k) {
+          const float2 p = pk[k], q = pk[(AY - k) % AY];
+          a[k] = make_float2(0.5f * (p.x + q.x), 0.5f * (p.y - q.y));
+          b[k] = make_float2(0.5f * (p.y + q.y), 0.5f * (q.x - p.x));
+        }
+        store_col<SH>(a, S, 0, z, y0, twny);
+        store_col<SH>(b, S, M, z, y0, twny);
       }
       if constexpr (M % 2 == 0 && M >= 2) {
         const int ph = xp<SH>(xrev<SH>(M / 2));
@@ -359,21 +384,20 @@ __device__ __forceinline__ void cols_inverse(float2* sm, const float2* __restric
     const int y0 = y0base + g;
     float2* rows = sm + g * SH::GSTRIDE;
     if (it == 0) {
+      // kx = 0 and kx = M invert to real columns a, b: one inverse DFT of
+      // A + i B gives a + i b (the imaginary parts of a and b, zero for a
+      // Hermitian spectrum, are not separated)
       const int p0 = xp<SH>(0);
       {
-        float2 xc[AY];
-        split_load<SH>(xc, S, 0, z, y0, twny);
+        float2 xa[AY], xb[AY];
+        load_col<SH>(xa, S, 0, z, y0, twny);
+        load_col<SH>(xb, S, M, z, y0, twny);
 #pragma unroll
-        for (int j = 0; j < AY; ++j) rows[j * RS + p0] = xc[j];
-      }
-      {
-        float2 xm[AY];
-        split_load<SH>(xm, S, M, z, y0, twny);
+        for (int k = 0; k < AY; ++k) xa[k] = make_float2(xa[k].x - xb[k].y, xa[k].y + xb[k].x);
+        dft<AY, +1>(xa);
 #pragma unroll
-        for (int j = 0; j < AY; ++j) {
-          const float x0 = rows[j * RS + p0].x;
-          rows[j * RS + p0] = make_float2(x0 + xm[j].x, x0 - xm[j].x);
-        }
+        for (int j = 0; j < AY; ++j)
+          rows[j * RS + p0] = make_float2(xa[j].x + xa[j].y, xa[j].x - xa[j].y);
       }
       if constexpr (M % 2 == 0 && M >= 2) {
         float2 xh[AY];

@@ -80,6 +80,19 @@ void plan_tables(const VolPlan& P, std::vector<int>* xrev, std::vector<TwTable>*
 // Planner (host only).  Returns false for shapes it cannot decompose.
 bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why);
 
+// Kernel families of the launch accounting and timing probes.
+enum KernelKind { KK_XY_FORWARD = 0, KK_Z = 1, KK_XY_INV_FWD = 2, KK_XY_INVERSE = 3,
+                  KK_OTHER = 4, KK_XY_PRODUCT = 5, KK_COUNT = 6 };
+
+// Timing family of a launch: the functor's own kFamily when it names one
+// (the RL product step, whose xy inverse+forward launches are timed apart
+// from the ratio step's), else the pass's default.
+template <class F, int DEF>
+constexpr int family_of() {
+  if constexpr (requires { F::kFamily; }) return F::kFamily;
+  else return DEF;
+}
+
 // Radices accepted for one register pass (must match dft_codelets.cuh).
 constexpr int kRadixSet[] = {16, 19, 17, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
 

@@ -11,6 +11,7 @@
 #include "engine.hpp"
 #include "ops.cuh"
 #include "passes_static.cuh"
+#include "passes_xy_tma.cuh"
 
 namespace clarity {
 
@@ -35,6 +36,53 @@ inline cudaError_t allow_smem_st(K kernel, int smem) {
     return cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   return cudaSuccess;
+}
+
+// The TMA XY pass (passes_xy_tma.cuh) serves epilogues with a staged form
+// unless CLARITY_XY_TMA=0.
+bool xy_tma_enabled();
+template <class F>
+constexpr bool xy_staged() {
+  if constexpr (requires { F::kStaged; }) return F::kStaged;
+  else return false;
+}
+
+// Tensor map of the spectrum S as floats {2*W*BY, NZ, KG, AY} with the box of
+// one XY tile.
+template <class SH>
+inline bool encode_s_map(TensorMap* tm, const float2* S) {
+  using X = st::XyTma<SH>;
+  const unsigned long long row = 2ull * SH::W * SH::BY;
+  const unsigned long long dim[4] = {row, (unsigned long long)SH::NZ,
+                                     (unsigned long long)SH::KG, (unsigned long long)SH::AY};
+  const unsigned long long stride[3] = {row * 4, row * 4 * SH::NZ,
+                                        row * 4 * SH::NZ * SH::KG};
+  const unsigned box[4] = {2u * X::BOXW, 1u, (unsigned)SH::KG, (unsigned)SH::AY};
+  return encode_tensor_f32_4d(tm, S, dim, stride, box);
+}
+
+// Launches the TMA XY pass when shape, epilogue and buffers allow it.
+template <class SH, bool FUSE, class F>
+inline bool try_xy_tma(const PlanEntry& pe, cudaStream_t st, const F& fn, const float2* S,
+                       int family, cudaError_t* err) {
+  using X = st::XyTma<SH>;
+  if constexpr (X::OK && xy_staged<F>()) {
+    if (!xy_tma_enabled()) return false;
+    TensorMap tm;
+    if (!encode_s_map<SH>(&tm, S)) return false;
+    auto k = st::ks_xy_tma<SH, F, FUSE>;
+    *err = allow_smem_st(k, X::SMEM);
+    if (*err != cudaSuccess) return true;
+    const st::Tables T = tables_of(pe);
+    note_launch_begin(family, st);
+    CLARITY_LAUNCH(k, X::BLOCKS, SH::THREADS, X::SMEM, st)(fn, tm, T);
+    note_launch_end(family, st);
+    *err = cudaGetLastError();
+    return true;
+  } else {
+    (void)pe; (void)st; (void)fn; (void)S; (void)family; (void)err;
+    return false;
+  }
 }
 
 // Kernel families that may use the specialised kernels: bit KIND of the
@@ -73,13 +121,15 @@ inline bool try_static(const PlanEntry& pe, cudaStream_t st, const F& fn, float2
       note_launch_end(KK_Z, st);
     }
   } else if constexpr (KIND == 2) {
+    if (try_xy_tma<SH, true>(pe, st, fn, Sa, family_of<F, KK_XY_INV_FWD>(), err)) return true;
     auto k = st::ks_xy_inv_fwd<SH, F>;
     *err = allow_smem_st(k, SH::XY_SMEM);
     if (*err != cudaSuccess) return true;
-    note_launch_begin(KK_XY_INV_FWD, st);
+    note_launch_begin(family_of<F, KK_XY_INV_FWD>(), st);
     CLARITY_LAUNCH(k, pe.P.xy_blocks, SH::THREADS, SH::XY_SMEM, st)(fn, Sa, T);
-    note_launch_end(KK_XY_INV_FWD, st);
+    note_launch_end(family_of<F, KK_XY_INV_FWD>(), st);
   } else {
+    if (try_xy_tma<SH, false>(pe, st, fn, Sb, KK_XY_INVERSE, err)) return true;
     auto k = st::ks_xy_inverse<SH, F>;
     *err = allow_smem_st(k, SH::XY_SMEM);
     if (*err != cudaSuccess) return true;

@@ -12,6 +12,9 @@
 #include <cstdint>
 
 #include "launch_macro.cuh"
+#ifndef CLARITY_HOST_EMULATION
+#include <cuda.h>  // CUtensorMap (the type only; the encoder is fetched at run time)
+#endif
 
 namespace clarity {
 
@@ -71,13 +74,48 @@ __device__ __forceinline__ void fence_smem_to_async() {
 __device__ __forceinline__ bool smem_aligned16(const void* p) {
   return (smem_u32(p) & 15u) == 0;
 }
+__device__ __forceinline__ bool smem_aligned128(const void* p) {
+  return (smem_u32(p) & 127u) == 0;
+}
 // Hint: bring [p, p+bytes) into L2 (p and bytes multiples of 16).
 __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// wait until this thread's committed bulk stores have read their shared source
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Tiled rank-4 tensor copies (TMA).  The map is a __grid_constant__ kernel
+// parameter; coordinates are element offsets, innermost first.  The caller
+// guarantees c0 * element size is a multiple of 16 bytes and, for stores,
+// that every coordinate is non-negative.
+using TensorMap = CUtensorMap;
+#define CLARITY_GRID_CONST const __grid_constant__
+__device__ __forceinline__ void tma_load_4d(void* dst, const TensorMap* tm, int c0, int c1,
+                                            int c2, int c3, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const TensorMap* tm, int c0, int c1, int c2,
+                                             int c3, const void* src) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group "
+      "[%0, {%1, %2, %3, %4}], [%5];" ::"l"(reinterpret_cast<uint64_t>(tm)),
+      "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
+      : "memory");
+}
 #else
 // Host emulation: copies happen immediately.
 inline bool smem_aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+inline bool smem_aligned128(const void* p) { return ((uintptr_t)p & 127u) == 0; }
 inline void prefetch_l2(const void*, uint32_t) {}
 inline void mbar_init(uint64_t* bar, uint32_t) { *bar = 0; }
 inline void mbar_arrive_expect_tx(uint64_t*, uint32_t) {}
@@ -89,7 +127,50 @@ inline void bulk_store(void* dst, const void* src, uint32_t bytes) {
   std::memcpy(dst, src, bytes);
 }
 inline void bulk_store_commit_and_wait() {}
+inline void bulk_commit() {}
+inline void bulk_wait_read_all() {}
 inline void fence_smem_to_async() {}
+// Host emulation of a rank-4 float tensor map and its tiled copies: elements
+// outside the tensor read as zero and are not written.
+#define CLARITY_GRID_CONST const
+struct TensorMap {
+  char* base;
+  unsigned long long dim[4];
+  unsigned long long stride[4];  // bytes; stride[0] = element size
+  unsigned box[4];
+};
+template <bool LOAD>
+inline void tma_copy_emu(char* smem, const TensorMap* tm, const int c[4]) {
+  size_t o = 0;
+  for (unsigned i3 = 0; i3 < tm->box[3]; ++i3)
+    for (unsigned i2 = 0; i2 < tm->box[2]; ++i2)
+      for (unsigned i1 = 0; i1 < tm->box[1]; ++i1)
+        for (unsigned i0 = 0; i0 < tm->box[0]; ++i0, o += 4) {
+          const long long g[4] = {(long long)c[0] + i0, (long long)c[1] + i1,
+                                  (long long)c[2] + i2, (long long)c[3] + i3};
+          bool in = true;
+          size_t off = 0;
+          for (int d = 0; d < 4; ++d) {
+            in = in && g[d] >= 0 && (unsigned long long)g[d] < tm->dim[d];
+            off += (size_t)g[d] * tm->stride[d];
+          }
+          if (LOAD) {
+            if (in) std::memcpy(smem + o, tm->base + off, 4);
+            else std::memset(smem + o, 0, 4);
+          } else if (in) {
+            std::memcpy(tm->base + off, smem + o, 4);
+          }
+        }
+}
+inline void tma_load_4d(void* dst, const TensorMap* tm, int c0, int c1, int c2, int c3,
+                        uint64_t*) {
+  const int c[4] = {c0, c1, c2, c3};
+  tma_copy_emu<true>(static_cast<char*>(dst), tm, c);
+}
+inline void tma_store_4d(const TensorMap* tm, int c0, int c1, int c2, int c3, const void* src) {
+  const int c[4] = {c0, c1, c2, c3};
+  tma_copy_emu<false>(const_cast<char*>(static_cast<const char*>(src)), tm, c);
+}
 inline int atomicExch(int* p, int v) {
   const int o = *p;
   *p = v;
@@ -105,6 +186,12 @@ __device__ __forceinline__ void prefetch_l2_range(const void* begin, size_t byte
   const uintptr_t hi = (b + bytes) & ~uintptr_t(15);
   if (hi > lo) prefetch_l2(reinterpret_cast<const void*>(lo), (uint32_t)(hi - lo));
 }
+
+// Encodes a rank-4 float32 tensor map (no interleave, no swizzle, zero fill):
+// dim innermost first, stride_bytes for dims 1..3, box extents.  False when
+// the driver rejects it (alignment, extents), so callers can fall back.
+bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
+                          const unsigned long long stride_bytes[3], const unsigned box[4]);
 
 // Bounded wait for phase `parity` of the barrier; false (and *err set) on
 // timeout.

@@ -91,8 +91,8 @@ CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
  * launched so far.  clarityx_timing_enable(1) makes every fused-pass launch
  * record a CUDA event pair on its stream; clarityx_timing_collect waits for
  * them and returns, per kernel family (0 xy-forward, 1 z, 2 xy-inverse+forward,
- * 3 xy-inverse, 4 other), the summed milliseconds and launch counts, then
- * clears the record. */
+ * 3 xy-inverse, 4 other, 5 xy-inverse+forward of the RL product step), the
+ * summed milliseconds and launch counts, then clears the record. */
 CLARITY_API long long clarityx_launch_count(void);
 CLARITY_API void clarityx_timing_enable(int on);
 CLARITY_API void clarityx_timing_collect(double *ms, long long *counts, int n);

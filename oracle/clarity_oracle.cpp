@@ -209,12 +209,43 @@ void wiener(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, T eps,
   if (out_work) std::memcpy(out_work, o.data(), sizeof(T) * w.n);
 }
 
+// Sampled Gaussian smoothing kernel for smoothed JVC, as a PSF of the work
+// box size: exp(-d^2 / (2 sigma^2)) per axis about the centre n/2 (a delta
+// along an axis with sigma <= 0), normalised to unit sum in double, then
+// rounded to float.  The reference has no definition to follow
+// (src/SmoothedJansenVanCittertDeconvolve.cxx:27-40 writes zeros); the CUDA
+// library builds the same kernel.
+std::vector<float> gauss_kernel(Dim3 wd, const double sigma[3]) {
+  const int n[3] = {wd.x, wd.y, wd.z};
+  std::vector<double> ax[3];
+  for (int d = 0; d < 3; ++d) {
+    ax[d].resize(n[d]);
+    const int c = n[d] / 2;
+    for (int i = 0; i < n[d]; ++i) {
+      const double t = i - c;
+      ax[d][i] = sigma[d] > 0 ? std::exp(-t * t / (2.0 * sigma[d] * sigma[d])) : (i == c ? 1.0 : 0.0);
+    }
+  }
+  double sum = 0;
+  for (int z = 0; z < n[2]; ++z)
+    for (int y = 0; y < n[1]; ++y)
+      for (int x = 0; x < n[0]; ++x) sum += ax[2][z] * ax[1][y] * ax[0][x];
+  std::vector<float> k((size_t)wd.n());
+  size_t o = 0;
+  for (int z = 0; z < n[2]; ++z)
+    for (int y = 0; y < n[1]; ++y)
+      for (int x = 0; x < n[0]; ++x) k[o++] = (float)(ax[2][z] * ax[1][y] * ax[0][x] / sum);
+  return k;
+}
+
 // JVC: src/JansenVanCittertDeconvolve.cxx:122-192 with the update of
 // :90-119 and A = max(unpadded image)/2 (:128-129, :324).  iterations <= 1
-// performs exactly one update (:167-173).
+// performs exactly one update (:167-173).  Smoothed JVC (interval > 0):
+// after every interval-th update the estimate on the work box is convolved
+// with gauss_kernel(sigma) (pad/shift as any PSF, then C2R(R2C(i) G / N)).
 template <class T, class S>
 void jvc(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
-         T* out_work) {
+         T* out_work, int interval = 0, const double* sigma = nullptr) {
   Work<T> w(in, id, kernel, kd);
   const long n = w.n;
   T mx = (T)in[0];
@@ -225,6 +256,15 @@ void jvc(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
   std::vector<oracle::cx<T>> otf(w.nc), tmp(w.nc);
   w.r2c(w.h.data(), otf.data());
   std::vector<T> i_k(w.g), o(n);
+  std::vector<oracle::cx<T>> gotf;
+  if (interval > 0) {
+    const std::vector<float> gk = gauss_kernel(w.wd, sigma);
+    std::vector<T> gpad(n);
+    const int sh[3] = {-w.wd.x / 2, -w.wd.y / 2, -w.wd.z / 2};
+    pad_shift<T, float>(gpad.data(), w.wd, gk.data(), w.wd, sh, (T)0);
+    gotf.resize(w.nc);
+    w.r2c(gpad.data(), gotf.data());
+  }
   const int total = iters > 1 ? iters : 1;
   for (int k = 0; k < total; k++) {
     convolve_otf<T>(w, i_k.data(), otf.data(), o.data(), tmp);
@@ -234,6 +274,10 @@ void jvc(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
       T val = i_k[j] + (gamma * (w.g[j] - o[j]));
       if (val < (T)0) val = (T)0;
       i_k[j] = val;
+    }
+    if (interval > 0 && (k + 1) % interval == 0) {
+      convolve_otf<T>(w, i_k.data(), gotf.data(), o.data(), tmp);
+      i_k.swap(o);
     }
   }
   clip<T, S>(out, id, i_k.data(), w.wd);
@@ -332,6 +376,20 @@ void oracle_jvc_f64(const float* in, int ix, int iy, int iz, const float* k,
                     double* work) {
   ORACLE_DIMS;
   jvc<double, float>(in, id, k, kd, out, iters, work);
+}
+void oracle_sjvc_f32(const float* in, int ix, int iy, int iz, const float* k,
+                     int kx, int ky, int kz, float* out, int iters, int interval,
+                     double sx, double sy, double sz, float* work) {
+  ORACLE_DIMS;
+  const double sg[3] = {sx, sy, sz};
+  jvc<float, float>(in, id, k, kd, out, iters, work, interval, sg);
+}
+void oracle_sjvc_f64(const float* in, int ix, int iy, int iz, const float* k,
+                     int kx, int ky, int kz, float* out, int iters, int interval,
+                     double sx, double sy, double sz, double* work) {
+  ORACLE_DIMS;
+  const double sg[3] = {sx, sy, sz};
+  jvc<double, float>(in, id, k, kd, out, iters, work, interval, sg);
 }
 void oracle_blind_f32(const float* in, int ix, int iy, int iz,
                       const float* k, int kx, int ky, int kz, float* out,

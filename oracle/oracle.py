@@ -70,6 +70,7 @@ class Oracle:
         i = C.c_int
         for name, extra in [("convolve", []), ("rl", [i, i]),
                             ("wiener", [C.c_float]), ("jvc", [i]),
+                            ("sjvc", [i, i, C.c_double, C.c_double, C.c_double]),
                             ("blind", [i, i])]:
             fn = getattr(L, f"oracle_{name}_f32")
             fn.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p] + extra + [C.c_void_p]
@@ -117,6 +118,10 @@ class Oracle:
 
     def jvc(self, img, psf, iters, precision="f32", work=False):
         return self._run("jvc", img, psf, [iters], precision, work)
+
+    def smoothed_jvc(self, img, psf, iters, interval, sigma_xyz, precision="f32", work=False):
+        sx, sy, sz = (float(v) for v in sigma_xyz)
+        return self._run("sjvc", img, psf, [iters, interval, sx, sy, sz], precision, work)
 
     def blind(self, img, psf, iters, precision="f32", sum_mode=SUM_DOUBLE, work=False):
         extra = [iters, sum_mode] if precision == "f32" else [iters]

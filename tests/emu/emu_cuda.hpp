@@ -38,7 +38,7 @@ struct Launcher {
         gDim = dim3((unsigned)g, 1, 1);
         void* p = nullptr;
         if (s) {
-          p = std::malloc(s);
+          p = std::aligned_alloc(128, (s + 127) / 128 * 128);  // as __align__(128)
           std::memset(p, 0xff, s);
         }
         smem_ptr = p;

@@ -1,7 +1,7 @@
 // emu_main.cpp -- TEST INFRASTRUCTURE: drives the library's public C API in
 // the CPU emulation build.
 //   emu_main <op> ix iy iz kx ky kz <param> image.raw psf.raw out.raw
-// op: convolve | rl | blind | jvc | wiener (param = iterations or epsilon).
+// op: convolve | rl | blind | jvc | sjvc | wiener (param = iterations or epsilon).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -44,7 +44,12 @@ int main(int argc, char** argv) {
                                                  (int)param);
   else if (op == "jvc")
     r = Clarity_JansenVanCittertDeconvolve(img.data(), id, psf.data(), kd, out.data(), (int)param);
-  else if (op == "convolve_noalloc")  // emulated device memory is host memory
+  else if (op == "sjvc") {  // smoothed JVC: interval 2, sigma (1.0, 1.5, 0.7)
+    float sx = 1.0f, sy = 1.5f, sz = 0.7f;
+    float* sig[3] = {&sx, &sy, &sz};
+    r = Clarity_SmoothedJansenVanCittertDeconvolve(img.data(), id, psf.data(), kd, out.data(),
+                                                   (unsigned)param, 2u, sig);
+  } else if (op == "convolve_noalloc")  // emulated device memory is host memory
     r = clarityx_convolve_noalloc(img.data(), id, psf.data(), kd, out.data(), nullptr);
   else if (op == "wiener")
     r = Clarity_WienerDeconvolve(img.data(), id, psf.data(), kd, out.data(), (float)param);
