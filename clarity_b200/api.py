@@ -55,8 +55,9 @@ EXTENSION_SYMBOLS = [
     "clarityx_wiener_device", "clarityx_ml_device", "clarityx_blind_ml_device",
     "clarityx_jvc_device", "clarityx_idivergence", "clarityx_plan_info",
     "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
-    "clarityx_convolve_noalloc",
+    "clarityx_convolve_noalloc", "clarityx_ml_batch_device", "clarityx_autotune",
 ]
+BATCH_GRAPH = 1  # CLARITYX_BATCH_GRAPH
 
 
 class ClarityError(RuntimeError):
@@ -137,6 +138,12 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_plan_info.restype = i
         L.clarityx_convolve_noalloc.argtypes = [vp, Dim3, vp, Dim3, vp, vp]
         L.clarityx_convolve_noalloc.restype = i
+        L.clarityx_ml_batch_device.argtypes = [i, C.POINTER(vp), C.POINTER(Dim3),
+                                               C.POINTER(vp), C.POINTER(Dim3),
+                                               C.POINTER(vp), i, i, vp]
+        L.clarityx_ml_batch_device.restype = i
+        L.clarityx_autotune.argtypes = [i]
+        L.clarityx_autotune.restype = None
         L.clarityx_launch_count.restype = C.c_longlong
         L.clarityx_timing_enable.argtypes = [i]
         L.clarityx_timing_enable.restype = None
@@ -350,3 +357,30 @@ def blind_ml_device(image, kernel, out, iterations, stream=None):
 
 def jvc_device(image, kernel, out, iterations, stream=None):
     return _dev("clarityx_jvc_device", image, kernel, out, [int(iterations)], stream)
+
+
+def ml_batch_device(images, kernels, outs, iterations, graph=True, stream=None):
+    """clarityx_ml_batch_device: Richardson-Lucy on lists of device tensors
+    (volumes of any sizes, one kernel each), run concurrently; with graph the
+    batch is captured into a CUDA graph and replayed on later identical
+    calls.  Asynchronous on `stream`."""
+    n = len(images)
+    if len(kernels) != n or len(outs) != n:
+        raise ValueError("images, kernels and outs must have the same length")
+    for t in list(images) + list(kernels) + list(outs):
+        if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+            raise ValueError("batch volumes must be contiguous float32 CUDA tensors")
+    vp = C.c_void_p
+    imgs = (vp * n)(*[t.data_ptr() for t in images])
+    kers = (vp * n)(*[t.data_ptr() for t in kernels])
+    outp = (vp * n)(*[t.data_ptr() for t in outs])
+    ids = (Dim3 * n)(*[dim3(t) for t in images])
+    kds = (Dim3 * n)(*[dim3(t) for t in kernels])
+    _check(load().clarityx_ml_batch_device(n, imgs, ids, kers, kds, outp, int(iterations),
+                                           BATCH_GRAPH if graph else 0, _stream_ptr(stream)))
+    return outs
+
+
+def autotune(on: bool = True) -> None:
+    """clarityx_autotune: time candidate plans on first use of a work box."""
+    load().clarityx_autotune(1 if on else 0)

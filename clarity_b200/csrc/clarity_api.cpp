@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <vector>
 #include <string>
 
 #include "../../include/clarity.h"
@@ -29,6 +30,7 @@ std::mutex g_mu;                 // guards registration state
 int g_refcount = 0;              // src/Clarity.cxx:41 (made thread-safe)
 int g_device = 0;
 Context* g_ctx = nullptr;
+bool g_autotune = false;         // applied to contexts created later too
 unsigned g_threads = 0;
 thread_local char g_last_error[512];
 
@@ -170,6 +172,7 @@ ClarityResult_t Clarity_Register(void) {
       return fail(CLARITY_INVALID_OPERATION,
                   std::string("device is not sm_100 class: ") + prop.name);
     g_ctx = new Context(g_device);
+    g_ctx->set_autotune(g_autotune);
     if (std::getenv("CLARITY_LOG"))
       std::fprintf(stderr, "clarity: device %d '%s', %zu MB\n", g_device, prop.name,
                    (size_t)(prop.totalGlobalMem >> 20));
@@ -403,6 +406,46 @@ ClarityResult_t clarityx_ml_device(const float* image, Clarity_Dim3 imageDim,
                          float* o) {
                        return clarity::run_rl(c, i, id, k, kd, o, iterations);
                      });
+}
+
+ClarityResult_t clarityx_ml_batch_device(int count, const float* const* images,
+                                         const Clarity_Dim3* imageDims,
+                                         const float* const* kernels,
+                                         const Clarity_Dim3* kernelDims, float* const* outs,
+                                         int iterations, int flags, void* stream) {
+  if (count < 0) return fail(CLARITY_INVALID_ARGUMENT, "count < 0");
+  if (count == 0) return CLARITY_SUCCESS;
+  if (!images || !imageDims || !kernels || !kernelDims || !outs)
+    return fail(CLARITY_INVALID_ARGUMENT, "NULL array");
+  std::vector<Dims> ids(count), kds(count);
+  for (int i = 0; i < count; ++i) {
+    if (!dims_ok(imageDims[i]) || !dims_ok(kernelDims[i]))
+      return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+    ids[i] = to_dims(imageDims[i]);
+    kds[i] = to_dims(kernelDims[i]);
+  }
+  Context* ctx;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx = g_ctx;
+  }
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device());
+  ctx->set_stream(static_cast<cudaStream_t>(stream));
+  Status s = clarity::run_rl_batch(*ctx, count, images, ids.data(), kernels, kds.data(), outs,
+                                   iterations, (flags & CLARITYX_BATCH_GRAPH) != 0);
+  ctx->set_stream(nullptr);
+  return report(s);
+}
+
+void clarityx_autotune(int on) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_autotune = on != 0;
+  if (g_ctx) {
+    std::lock_guard<std::mutex> lk2(g_ctx->mu);
+    g_ctx->set_autotune(g_autotune);
+  }
 }
 
 ClarityResult_t clarityx_blind_ml_device(const float* image, Clarity_Dim3 imageDim,

@@ -82,11 +82,33 @@ constexpr cs_pair root_cs(long k, long n) {
 }
 
 // ------------------------------------------------------------ complex ops
+// Complex add and subtract use sm_100's paired FP32 add (one FADD2 per complex
+// add instead of two FADDs; each lane rounds exactly as a scalar add), unless
+// CLARITY_NO_F32X2 is defined or the code is compiled for the host.
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && !defined(CLARITY_NO_F32X2)
+#define CLARITY_F32X2 1
+#endif
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+#ifdef CLARITY_F32X2
+  return __fadd2_rn(a, b);
+#else
   return make_float2(a.x + b.x, a.y + b.y);
+#endif
 }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+#ifdef CLARITY_F32X2
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+#else
   return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+// a + DIR*i*b, in scalar adds (the lane swap would cost moves in paired form)
+template <int DIR>
+__device__ __forceinline__ float2 cadd_diri(float2 a, float2 b) {
+  if constexpr (DIR < 0)
+    return make_float2(a.x + b.y, a.y - b.x);
+  else
+    return make_float2(a.x - b.y, a.y + b.x);
 }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -170,8 +192,8 @@ struct DFT<3, DIR> {
     float2 t = make_float2(a0.x + c * s.x, a0.y + c * s.y);
     float2 jd = make_float2(-sn * d.y, sn * d.x);
     v[0] = cadd(a0, s);
-    v[1] = cadd(t, jd);
-    v[2] = csub(t, jd);
+    v[1] = make_float2(t.x + jd.x, t.y + jd.y);
+    v[2] = make_float2(t.x - jd.x, t.y - jd.y);
   }
 };
 
@@ -180,11 +202,10 @@ struct DFT<4, DIR> {
   __device__ __forceinline__ static void run(float2* v) {
     float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
     float2 s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
-    float2 j = mul_diri<DIR>(d13);
     v[0] = cadd(s02, s13);
-    v[1] = cadd(d02, j);
+    v[1] = cadd_diri<DIR>(d02, d13);
     v[2] = csub(s02, s13);
-    v[3] = csub(d02, j);
+    v[3] = cadd_diri<-DIR>(d02, d13);
   }
 };
 
@@ -218,9 +239,8 @@ struct DFTPrime {
         S.y += s * b[t].y;
       });
       // X[k] = C + DIR*i*S ; X[N-k] = C - DIR*i*S
-      float2 jS = mul_diri<DIR>(S);
-      out[k] = cadd(C, jS);
-      out[N - k] = csub(C, jS);
+      out[k] = cadd_diri<DIR>(C, S);
+      out[N - k] = cadd_diri<-DIR>(C, S);
     });
     static_for<N>([&](auto ki) {
       constexpr int k = decltype(ki)::value;

@@ -26,6 +26,12 @@
 
 namespace clarity {
 
+#define CL_TRY(expr)              \
+  do {                            \
+    Status s_ = (expr);           \
+    if (!s_.ok()) return s_;      \
+  } while (0)
+
 // ------------------------------------------------------------------ errors
 Status status_from_cuda(cudaError_t e, const char* what) {
   Status s;
@@ -75,9 +81,14 @@ static cudaEvent_t take_event() {
   return e;
 }
 
+// Set while a batch is captured into a graph: launches are counted, but no
+// timing events are recorded into the capture.
+static thread_local bool t_capturing = false;
+void set_capturing(bool on) { t_capturing = on; }
+
 void note_launch_begin(int kind, cudaStream_t st) {
   g_launches.fetch_add(1);
-  if (!g_timing.load()) return;
+  if (!g_timing.load() || t_capturing) return;
   std::lock_guard<std::mutex> lk(g_timing_mu);
   cudaEvent_t e = take_event();
   cudaEventRecord(e, st);
@@ -85,7 +96,7 @@ void note_launch_begin(int kind, cudaStream_t st) {
 }
 
 void note_launch_end(int kind, cudaStream_t st) {
-  if (!g_timing.load()) return;
+  if (!g_timing.load() || t_capturing) return;
   std::lock_guard<std::mutex> lk(g_timing_mu);
   cudaEvent_t e = take_event();
   cudaEventRecord(e, st);
@@ -314,6 +325,8 @@ Context::Context(int device) : device_(device) {
 Context::~Context() {
   cudaSetDevice(device_);
   release_workspaces();
+  for (cudaStream_t b : bstreams_) cudaStreamDestroy(b);
+  bstreams_.clear();
   for (auto& kv : plans_) {
     cudaFree(kv.second->tw);
     cudaFree(kv.second->xrev);
@@ -323,30 +336,50 @@ Context::~Context() {
   if (stream_) cudaStreamDestroy(stream_);
 }
 
-void Context::release_workspaces() {
-  Workspace& w = ws_;
+static void free_workspace(Workspace& w) {
   cudaFree(w.S); cudaFree(w.H); cudaFree(w.u); cudaFree(w.img); cudaFree(w.ker);
   cudaFree(w.partial); cudaFree(w.dscal); cudaFree(w.fscal); cudaFree(w.iscal);
   cudaFree(w.HG);
   w = Workspace();
 }
 
-Status Context::plan(const Dims& wd, const PlanEntry** out) {
-  auto key = std::make_tuple(wd.x, wd.y, wd.z);
-  auto it = plans_.find(key);
-  if (it != plans_.end()) {
-    *out = it->second.get();
-    return Status::Ok();
+void Context::release_workspaces() {
+  // graphs hold workspace addresses: they go first
+  for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+  graphs_.clear();
+  free_workspace(ws_);
+  for (auto& w : slots_) free_workspace(*w);
+  slots_.clear();
+}
+
+Status Context::batch_stream(int i, cudaStream_t* out) {
+  while ((int)bstreams_.size() <= i) {
+    cudaStream_t b = nullptr;
+    CL_CHECK(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+    bstreams_.push_back(b);
   }
+  *out = bstreams_[i];
+  return Status::Ok();
+}
+
+cudaGraphExec_t Context::find_graph(const std::vector<unsigned long long>& key) const {
+  for (const auto& g : graphs_)
+    if (g.key == key) return g.exec;
+  return nullptr;
+}
+
+void Context::add_graph(std::vector<unsigned long long> key, cudaGraphExec_t g) {
+  constexpr size_t kMaxGraphs = 8;  // oldest first out
+  if (graphs_.size() >= kMaxGraphs) {
+    cudaGraphExecDestroy(graphs_.front().exec);
+    graphs_.erase(graphs_.begin());
+  }
+  graphs_.push_back(GraphEntry{std::move(key), g});
+}
+
+Status Context::build_entry(const VolPlan& P0, std::unique_ptr<PlanEntry>* out) {
   auto pe = std::make_unique<PlanEntry>();
-  std::string why;
-  if (!make_plan(wd.x, wd.y, wd.z, &pe->P, &why)) {
-    Status s;
-    s.code = CLARITY_INVALID_ARGUMENT;
-    s.msg = "unsupported work box " + std::to_string(wd.x) + "x" +
-            std::to_string(wd.y) + "x" + std::to_string(wd.z) + ": " + why;
-    return s;
-  }
+  pe->P = P0;
   const VolPlan& P = pe->P;
   CL_CHECK(dev_alloc((void**)&pe->tw, sizeof(float2) * P.twiddle_count));
   CL_CHECK(dev_alloc((void**)&pe->xrev, sizeof(int) * std::max(P.xrev_count, 1)));
@@ -366,6 +399,38 @@ Status Context::plan(const Dims& wd, const PlanEntry** out) {
   CL_CHECK(cudaGetLastError());
   CL_CHECK(cudaStreamSynchronize(st));
   cudaFree(dtabs);
+  *out = std::move(pe);
+  return Status::Ok();
+}
+
+static void free_entry(PlanEntry& pe) {
+  cudaFree(pe.tw);
+  cudaFree(pe.xrev);
+  cudaFree(pe.err);
+}
+
+Status Context::plan(const Dims& wd, const PlanEntry** out) {
+  auto key = std::make_tuple(wd.x, wd.y, wd.z);
+  auto it = plans_.find(key);
+  if (it != plans_.end()) {
+    *out = it->second.get();
+    return Status::Ok();
+  }
+  std::unique_ptr<PlanEntry> pe;
+  if (autotune_) {
+    CL_TRY(tune(wd, &pe));
+  } else {
+    VolPlan P;
+    std::string why;
+    if (!make_plan(wd.x, wd.y, wd.z, &P, &why)) {
+      Status s;
+      s.code = CLARITY_INVALID_ARGUMENT;
+      s.msg = "unsupported work box " + std::to_string(wd.x) + "x" +
+              std::to_string(wd.y) + "x" + std::to_string(wd.z) + ": " + why;
+      return s;
+    }
+    CL_TRY(build_entry(P, &pe));
+  }
   *out = pe.get();
   plans_[key] = std::move(pe);
   return Status::Ok();
@@ -397,9 +462,26 @@ static Status ensure(T** p, long long* cap, long long need) {
   return Status::Ok();
 }
 
+static Status fill_workspace(Workspace& w, const PlanEntry& pe, const Dims& img,
+                             const Dims& ker);
+
 Status Context::workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
                           Workspace** out) {
-  Workspace& w = ws_;
+  CL_TRY(fill_workspace(ws_, pe, img, ker));
+  *out = &ws_;
+  return Status::Ok();
+}
+
+Status Context::workspace_slot(int slot, const PlanEntry& pe, const Dims& img, const Dims& ker,
+                               Workspace** out) {
+  while ((int)slots_.size() <= slot) slots_.push_back(std::make_unique<Workspace>());
+  CL_TRY(fill_workspace(*slots_[slot], pe, img, ker));
+  *out = slots_[slot].get();
+  return Status::Ok();
+}
+
+static Status fill_workspace(Workspace& w, const PlanEntry& pe, const Dims& img,
+                             const Dims& ker) {
   const VolPlan& P = pe.P;
   long long sc = w.spec_cap;
   Status s;
@@ -431,18 +513,12 @@ Status Context::workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
   if (!w.dscal) CL_CHECK(dev_alloc((void**)&w.dscal, sizeof(double) * 16));
   if (!w.fscal) CL_CHECK(dev_alloc((void**)&w.fscal, sizeof(float) * 16));
   if (!w.iscal) CL_CHECK(dev_alloc((void**)&w.iscal, sizeof(int) * 16));
-  *out = &w;
   return Status::Ok();
 }
 
 // Launch wrappers are instantiated in the kern_*.cu translation units.
 CLARITY_EXTERN_LAUNCHES
 
-#define CL_TRY(expr)              \
-  do {                            \
-    Status s_ = (expr);           \
-    if (!s_.ok()) return s_;      \
-  } while (0)
 
 static PaddedSrc padded(const float* src, Dims sd, Dims wd, int sx, int sy,
                         int sz) {
@@ -496,6 +572,91 @@ static Status reduce_sum_into(Context& ctx, const float* a, long long n,
   count_small();
   CLARITY_LAUNCH(k_finish_sum, 1, 256, 0, st)(partial, kReduceBlocks, dout);
   CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+// Autotuner: builds the planner's best few tilings of the box and times one
+// Richardson-Lucy iteration's passes (z, ratio, z, product) with each on
+// zero-filled scratch volumes; the fastest plan is kept.
+Status Context::tune(const Dims& wd, std::unique_ptr<PlanEntry>* out) {
+  VolPlan cand[4];
+  std::string why;
+  const int nc = make_plan_candidates(wd.x, wd.y, wd.z, cand, 4, &why);
+  if (nc == 0) {
+    Status s;
+    s.code = CLARITY_INVALID_ARGUMENT;
+    s.msg = "unsupported work box " + std::to_string(wd.x) + "x" + std::to_string(wd.y) +
+            "x" + std::to_string(wd.z) + ": " + why;
+    return s;
+  }
+  if (nc == 1) return build_entry(cand[0], out);
+  long long spec = 0, parts = kReduceBlocks;
+  for (int c = 0; c < nc; ++c) {
+    spec = std::max(spec, cand[c].spec_elems);
+    parts = std::max<long long>({parts, (long long)cand[c].xy_blocks,
+                                 (long long)cand[c].nz * cand[c].By});
+  }
+  float2* S = nullptr;
+  float* u = nullptr;
+  double* partial = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::unique_ptr<PlanEntry> best;
+  float best_ms = 0.f;
+  Status st = Status::Ok();
+  cudaStream_t sm = exec_stream();
+  auto run = [&]() -> Status {
+    CL_CHECK(dev_alloc((void**)&S, sizeof(float2) * (size_t)spec));
+    CL_CHECK(dev_alloc((void**)&u, sizeof(float) * (size_t)wd.n()));
+    CL_CHECK(dev_alloc((void**)&partial, sizeof(double) * (size_t)parts));
+    CL_CHECK(cudaMemsetAsync(S, 0, sizeof(float2) * (size_t)spec, sm));
+    CL_CHECK(cudaMemsetAsync(u, 0, sizeof(float) * (size_t)wd.n(), sm));
+    CL_CHECK(cudaEventCreate(&e0));
+    CL_CHECK(cudaEventCreate(&e1));
+    const ImageSrc g{u, wd.x, wd.y, wd.z};
+    const WorkVol wv{wd.x, wd.y, wd.z};
+    for (int c = 0; c < nc; ++c) {
+      std::unique_ptr<PlanEntry> pe;
+      CL_TRY(build_entry(cand[c], &pe));
+      const int xm = pe->P.xmode;
+      auto iteration = [&]() -> Status {
+        CL_TRY(z_pass(*this, *pe, ModOTF{S, 1.f}, S, S));
+        CL_TRY(xy_inv_fwd(*this, *pe, MidRLRatio{g, xm}, S));
+        CL_TRY(z_pass(*this, *pe, ModOTF{S, 1.f}, S, S));
+        EpiRLProduct epi{};
+        epi.cur = u; epi.g = g; epi.scale = nullptr; epi.unew = u; epi.partial = partial;
+        epi.w = wv; epi.xmode = xm; epi.acc = 0.0; epi.nblocks = nullptr;
+        CL_TRY(xy_inv_fwd(*this, *pe, epi, S));
+        return Status::Ok();
+      };
+      CL_TRY(iteration());  // warm-up (first launches configure the kernels)
+      CL_CHECK(cudaEventRecord(e0, sm));
+      for (int r = 0; r < 3; ++r) CL_TRY(iteration());
+      CL_CHECK(cudaEventRecord(e1, sm));
+      CL_CHECK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CL_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+      if (!best || ms < best_ms) {
+        if (best) free_entry(*best);
+        best = std::move(pe);
+        best_ms = ms;
+      } else {
+        free_entry(*pe);
+      }
+    }
+    return Status::Ok();
+  };
+  st = run();
+  cudaStreamSynchronize(sm);
+  cudaFree(S);
+  cudaFree(u);
+  cudaFree(partial);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (!st.ok()) {
+    if (best) free_entry(*best);
+    return st;
+  }
+  *out = std::move(best);
   return Status::Ok();
 }
 
@@ -585,12 +746,10 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
   return Status::Ok();
 }
 
-Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
-              Dims kd, float* out, int iters) {
-  const PlanEntry* pe;
-  Workspace* ws;
-  Dims wd;
-  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+// One Richardson-Lucy solve on prepared plan and workspace, enqueued on
+// ctx.exec_stream(): OTF, the iterations, the clipped result.
+static Status rl_solve(Context& ctx, const PlanEntry& pe, Workspace& ws, const float* img,
+                       Dims id, const float* ker, Dims kd, Dims wd, float* out, int iters) {
   cudaStream_t st = ctx.exec_stream();
   if (iters <= 0) {
     // the reference leaves the output unwritten; return the input image
@@ -599,12 +758,130 @@ Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
     CL_CHECK(cudaGetLastError());
     return Status::Ok();
   }
-  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
-  CL_TRY(rl_core(ctx, *pe, *ws, img, id, wd, iters, true));
+  CL_TRY(make_otf(ctx, pe, ker, kd, wd, ws.H, nullptr));
+  CL_TRY(rl_core(ctx, pe, ws, img, id, wd, iters, true));
   count_small();
-  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws->u, wd.x, wd.y, out, id.x, id.y, id.z,
-                                        ws->fscal);
+  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws.u, wd.x, wd.y, out, id.x, id.y, id.z,
+                                                    ws.fscal);
   CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+// Runs a scope's enqueues on another stream of the context.
+struct StreamScope {
+  Context& ctx;
+  cudaStream_t saved;
+  StreamScope(Context& c, cudaStream_t s) : ctx(c), saved(c.user_stream()) { c.set_stream(s); }
+  ~StreamScope() { ctx.set_stream(saved); }
+};
+
+Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
+              Dims kd, float* out, int iters) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  return rl_solve(ctx, *pe, *ws, img, id, ker, kd, wd, out, iters);
+}
+
+// Batched Richardson-Lucy.  Set-up (plans, possibly autotuned, and one
+// workspace per volume) happens first, outside any capture; then every
+// volume's solve is issued on batch stream i % nstreams, forked from and
+// joined back to the caller's stream by events, either directly or captured
+// into one CUDA graph that later calls with the same volumes replay.
+Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* ids,
+                    const float* const* kers, const Dims* kds, float* const* outs, int iters,
+                    bool use_graph) {
+  if (n <= 0) return Status::Ok();
+#ifdef CLARITY_HOST_EMULATION
+  use_graph = false;  // the emulation runs kernels as they are issued
+#endif
+  constexpr int kBatchStreams = 8;
+  const int ns = std::min(n, kBatchStreams);
+  std::vector<const PlanEntry*> pes(n);
+  std::vector<Workspace*> wss(n);
+  std::vector<Dims> wds(n);
+  std::vector<cudaStream_t> bs(ns);
+  for (int i = 0; i < n; ++i) {
+    if (!imgs[i] || !kers[i] || !outs[i]) {
+      Status s;
+      s.code = CLARITY_INVALID_ARGUMENT;
+      s.msg = "batch volume " + std::to_string(i) + ": NULL pointer";
+      return s;
+    }
+    wds[i] = work_dims(ids[i], kds[i]);
+    CL_TRY(ctx.plan(wds[i], &pes[i]));
+    CL_TRY(ctx.workspace_slot(i, *pes[i], ids[i], kds[i], &wss[i]));
+  }
+  for (int j = 0; j < ns; ++j) CL_TRY(ctx.batch_stream(j, &bs[j]));
+  const cudaStream_t origin = ctx.exec_stream();
+  std::vector<unsigned long long> key;
+  key.push_back((unsigned long long)n);
+  key.push_back((unsigned long long)iters);
+  key.push_back((unsigned long long)(uintptr_t)origin);
+  for (int i = 0; i < n; ++i) {
+    for (const void* p : {(const void*)imgs[i], (const void*)kers[i], (const void*)outs[i],
+                          (const void*)wss[i]->S, (const void*)wss[i]->H,
+                          (const void*)wss[i]->u, (const void*)pes[i]})
+      key.push_back((unsigned long long)(uintptr_t)p);
+    key.push_back(((unsigned long long)ids[i].x << 42) | ((unsigned long long)ids[i].y << 21) |
+                  (unsigned long long)ids[i].z);
+    key.push_back(((unsigned long long)kds[i].x << 42) | ((unsigned long long)kds[i].y << 21) |
+                  (unsigned long long)kds[i].z);
+  }
+  if (use_graph) {
+    if (cudaGraphExec_t g = ctx.find_graph(key)) {
+      CL_CHECK(cudaGraphLaunch(g, origin));
+      return Status::Ok();
+    }
+  }
+  auto issue = [&]() -> Status {
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join(ns, nullptr);
+    Status st = Status::Ok();
+    auto body = [&]() -> Status {
+      CL_CHECK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+      for (int j = 0; j < ns; ++j)
+        CL_CHECK(cudaEventCreateWithFlags(&join[j], cudaEventDisableTiming));
+      CL_CHECK(cudaEventRecord(fork, origin));
+      for (int j = 0; j < ns; ++j) CL_CHECK(cudaStreamWaitEvent(bs[j], fork, 0));
+      for (int i = 0; i < n; ++i) {
+        StreamScope scope(ctx, bs[i % ns]);
+        CL_TRY(rl_solve(ctx, *pes[i], *wss[i], imgs[i], ids[i], kers[i], kds[i], wds[i],
+                        outs[i], iters));
+      }
+      for (int j = 0; j < ns; ++j) {
+        CL_CHECK(cudaEventRecord(join[j], bs[j]));
+        CL_CHECK(cudaStreamWaitEvent(origin, join[j], 0));
+      }
+      return Status::Ok();
+    };
+    st = body();
+    if (fork) cudaEventDestroy(fork);
+    for (cudaEvent_t e : join)
+      if (e) cudaEventDestroy(e);
+    return st;
+  };
+  if (!use_graph) return issue();
+#ifndef CLARITY_HOST_EMULATION
+  CL_CHECK(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal));
+  set_capturing(true);
+  Status st = issue();
+  set_capturing(false);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(origin, &graph);
+  if (!st.ok()) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  CL_CHECK(ce);
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  CL_CHECK(ie);
+  ctx.add_graph(std::move(key), exec);
+  CL_CHECK(cudaGraphLaunch(exec, origin));
+#endif
   return Status::Ok();
 }
 

@@ -69,11 +69,25 @@ class Context {
   int device() const { return device_; }
   cudaStream_t stream() const { return stream_; }
   void set_stream(cudaStream_t s) { user_stream_ = s; }
+  cudaStream_t user_stream() const { return user_stream_; }
   cudaStream_t exec_stream() const { return user_stream_ ? user_stream_ : stream_; }
 
   Status plan(const Dims& work, const PlanEntry** out);
   Status workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
                    Workspace** out);
+  // Workspace of batch slot `slot` (one per volume of a batched call).
+  Status workspace_slot(int slot, const PlanEntry& pe, const Dims& img, const Dims& ker,
+                        Workspace** out);
+  // Stream i of the batch stream pool (created on first use).
+  Status batch_stream(int i, cudaStream_t* out);
+  // Instantiated CUDA graph of a batched call, looked up by the call's
+  // pointers and sizes (nullptr when absent); add_graph takes ownership.
+  cudaGraphExec_t find_graph(const std::vector<unsigned long long>& key) const;
+  void add_graph(std::vector<unsigned long long> key, cudaGraphExec_t g);
+  // With autotuning on, the first plan of a work box times the planner's
+  // candidate tilings on the device and keeps the fastest.
+  void set_autotune(bool on) { autotune_ = on; }
+  bool autotune() const { return autotune_; }
   void release_workspaces();
   // Reads and clears every plan's device error word (synchronous).
   Status check_device_errors();
@@ -84,8 +98,18 @@ class Context {
   int device_;
   cudaStream_t stream_ = nullptr;
   cudaStream_t user_stream_ = nullptr;
+  Status build_entry(const VolPlan& P, std::unique_ptr<PlanEntry>* out);
+  Status tune(const Dims& wd, std::unique_ptr<PlanEntry>* out);
   std::map<std::tuple<int, int, int>, std::unique_ptr<PlanEntry>> plans_;
   Workspace ws_;
+  std::vector<std::unique_ptr<Workspace>> slots_;
+  std::vector<cudaStream_t> bstreams_;
+  struct GraphEntry {
+    std::vector<unsigned long long> key;
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs_;
+  bool autotune_ = false;
 };
 
 // ----------------------------------------------------------- algorithms
@@ -97,6 +121,13 @@ Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
                   Dims kd, float* out, float eps);
 Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
               Dims kd, float* out, int iters);
+// Richardson-Lucy on n independent volumes of any sizes (device pointers):
+// each volume has its own plan and workspace, volumes run concurrently on the
+// batch stream pool, and with use_graph the whole batch is captured into one
+// CUDA graph (replayed when the same batch is run again).
+Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* ids,
+                    const float* const* kers, const Dims* kds, float* const* outs, int iters,
+                    bool use_graph);
 Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
                  Dims kd, float* out, int iters);
 Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
@@ -115,6 +146,7 @@ void set_last_error(const char* msg);
 // on the launching stream.
 void note_launch_begin(int kind, cudaStream_t st);
 void note_launch_end(int kind, cudaStream_t st);
+void set_capturing(bool on);
 long long launch_count();
 int static_family_mask();
 void timing_enable(bool on);

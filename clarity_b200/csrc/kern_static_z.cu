@@ -1,4 +1,7 @@
 // kern_static_z.cu -- compile-time specialised pass kernels (static_dispatch.cuh).
+// The z pass keeps scalar complex adds: measured faster than paired FP32
+// adds here (its DFT chains are latency-bound), unlike the XY passes.
+#define CLARITY_NO_F32X2 1
 #include "static_dispatch.cuh"
 
 namespace clarity {

@@ -1,4 +1,7 @@
 // kern_z.cu -- explicit instantiations of the fused pass kernels (see launch.cuh).
+// The z pass keeps scalar complex adds: measured faster than paired FP32
+// adds here (its DFT chains are latency-bound), unlike the XY passes.
+#define CLARITY_NO_F32X2 1
 #include "launch.cuh"
 
 namespace clarity {

@@ -391,9 +391,22 @@ struct ModOTF {
                         off + chunk <= total ? chunk : total - off);
   }
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
+#ifdef PROBE_NOH
+    const float2 h = make_float2(1.f, 1e-3f * (float)(idx & 7));
+#else
     const float2 h = __ldg(&H[idx]);
+#endif
     const float f = scale2 ? scale * *scale2 : scale;
     return make_float2(f * (v.x * h.x - v.y * h.y), f * (v.x * h.y + v.y * h.x));
+  }
+  // the same operation with the deferred factor read once (per thread)
+  __device__ __forceinline__ ModOTF resolved() const {
+    ModOTF r = *this;
+    if (scale2) {
+      r.scale = scale * __ldg(scale2);
+      r.scale2 = nullptr;
+    }
+    return r;
   }
 };
 
@@ -418,6 +431,7 @@ struct ModWiener {
     const float a = h.x * f, b = -h.y * f;
     return make_float2(scale * (a * v.x - b * v.y), scale * (a * v.y + b * v.x));
   }
+  __device__ __forceinline__ ModWiener resolved() const { return *this; }
 };
 
 struct ModForward {
@@ -425,6 +439,7 @@ struct ModForward {
   int zn = 1 << 30;
   __device__ __forceinline__ void prefetch_tile(unsigned, int, int, int) const {}
   __device__ __forceinline__ float2 apply(long long, float2 v) const { return v; }
+  __device__ __forceinline__ ModForward resolved() const { return *this; }
 };
 
 }  // namespace clarity

@@ -505,6 +505,7 @@ __device__ __forceinline__ void z_mod_pass(float2* sm, const Mod& mod, long long
   constexpr int R = A::radix(S);
   constexpr int nblk = A::n / R;
   constexpr int total = SH::BW * nblk;
+  const Mod m = mod.resolved();
 #pragma unroll 1
   for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
     const int l0 = f % SH::BW;
@@ -515,7 +516,7 @@ __device__ __forceinline__ void z_mod_pass(float2* sm, const Mod& mod, long long
     for (int t = 0; t < R; ++t) v[t] = sm[base + t * SH::BW];
     dft<R, -1>(v);
 #pragma unroll
-    for (int t = 0; t < R; ++t) v[t] = mod.apply(gbase + base + t * SH::BW, v[t]);
+    for (int t = 0; t < R; ++t) v[t] = m.apply(gbase + base + t * SH::BW, v[t]);
     dft<R, +1>(v);
 #pragma unroll
     for (int t = 0; t < R; ++t) sm[base + t * SH::BW] = v[t];
@@ -709,6 +710,7 @@ __device__ __forceinline__ void z2_last(float2* sm, const Mod& mod, unsigned gba
   constexpr int R = A::radix(S);
   constexpr int nblk = A::n / R;
   constexpr int total = SH::BW * nblk;
+  const Mod m = mod.resolved();
 #pragma unroll 1
   for (int f = threadIdx.x; f < total; f += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
     const int l0 = f % SH::BW;
@@ -724,7 +726,7 @@ __device__ __forceinline__ void z2_last(float2* sm, const Mod& mod, unsigned gba
       for (int t = 0; t < R; ++t) out[g0 + t * SH::BW] = v[t];
     } else {
 #pragma unroll
-      for (int t = 0; t < R; ++t) v[t] = mod.apply(g0 + t * SH::BW, v[t]);
+      for (int t = 0; t < R; ++t) v[t] = m.apply(g0 + t * SH::BW, v[t]);
       dft<R, +1>(v);
 #pragma unroll
       for (int t = 0; t < R; ++t) sm[sbase + t * SH::ZS] = v[t];

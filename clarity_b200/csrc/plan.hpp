@@ -79,6 +79,9 @@ void plan_tables(const VolPlan& P, std::vector<int>* xrev, std::vector<TwTable>*
 
 // Planner (host only).  Returns false for shapes it cannot decompose.
 bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why);
+// Up to max_out (<= 8) tilings of the box, best model score first (the first
+// is make_plan's); the autotuner times them.  Returns how many.
+int make_plan_candidates(int nx, int ny, int nz, VolPlan* out, int max_out, std::string* why);
 
 // Kernel families of the launch accounting and timing probes.
 enum KernelKind { KK_XY_FORWARD = 0, KK_Z = 1, KK_XY_INV_FWD = 2, KK_XY_INVERSE = 3,

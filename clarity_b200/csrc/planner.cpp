@@ -61,7 +61,34 @@ static int ctz(int v) {
 static constexpr int kSmemMax = 200 * 1024;
 static constexpr int kSmemPerSM = 228 * 1024;
 
+// Fills the offsets of a chosen tiling (spectrum size, twiddle layout);
+// false when 32-bit offsets would not address the box.
+static bool finalize_plan(VolPlan& P, std::string* why) {
+  const long long spec = (long long)P.Ay * P.KG * P.nz * P.By * P.W;
+  if ((long long)P.nx * P.ny * P.nz >= (1ll << 31) || spec >= (1ll << 31)) {
+    if (why) *why = "work box of 2^31 voxels or more";
+    return false;
+  }
+  P.xy_threads = 256;
+  P.z_threads = 256;
+  P.spec_elems = spec;
+  int off = 0;
+  P.ax.tw_off = off; off += std::max(P.M, 1);
+  P.ayB.tw_off = off; off += std::max(P.By, 1);
+  P.az.tw_off = off; off += std::max(P.nz, 1);
+  P.tw_r2c_off = off; off += P.M / 2 + 1;
+  P.tw_ny_off = off; off += P.ny;
+  P.twiddle_count = off;
+  P.xrev_off = 0;
+  P.xrev_count = P.M;
+  return true;
+}
+
 bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
+  return make_plan_candidates(nx, ny, nz, out, 1, why) > 0;
+}
+
+int make_plan_candidates(int nx, int ny, int nz, VolPlan* out, int max_out, std::string* why) {
   VolPlan P;
   std::memset(&P, 0, sizeof(P));
   P.nx = nx; P.ny = ny; P.nz = nz;
@@ -89,9 +116,14 @@ bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
     if (rs % 2 == 0) rs += 1;
     P.rowStride = rs;
   }
-  double best_score = -1e300;
-  VolPlan best = P;
-  bool found = false;
+  // the max_out best-scoring tilings, best first (insertion into a fixed
+  // array: planning allocates nothing)
+  constexpr int kMaxCand = 8;
+  if (max_out > kMaxCand) max_out = kMaxCand;
+  if (max_out < 1) max_out = 1;
+  VolPlan cand[kMaxCand];
+  double cscore[kMaxCand];
+  int ncand = 0;
   // candidate Ay: 1 and every register radix (fixed array: planning
   // allocates nothing)
   int ays[1 + sizeof(kRadixSet) / sizeof(kRadixSet[0])];
@@ -125,47 +157,37 @@ bool make_plan(int nx, int ny, int nz, VolPlan* out, std::string* why) {
         score -= 4.0 * ((double)KG * W / P.XS - 1.0);
         score -= 0.05 * std::abs(ay - 16);
         score -= 0.02 * G;  // prefer fewer rows per tile at equal merit
-        if (score > best_score) {
-          best_score = score;
-          best = P;
-          best.Ay = ay; best.By = by; best.G = G; best.W = W; best.KG = KG;
-          best.ayB = ab;
-          best.xy_smem = (int)xysm;
-          best.z_smem = (int)zsm;
-          best.xy_blocks = (int)xy_blocks;
-          best.z_blocks = (int)z_blocks;
-          found = true;
+        int pos = ncand;
+        while (pos > 0 && score > cscore[pos - 1]) --pos;
+        if (pos < max_out) {
+          const int last = std::min(ncand, max_out - 1);
+          for (int q = last; q > pos; --q) {
+            cand[q] = cand[q - 1];
+            cscore[q] = cscore[q - 1];
+          }
+          VolPlan c = P;
+          c.Ay = ay; c.By = by; c.G = G; c.W = W; c.KG = KG;
+          c.ayB = ab;
+          c.xy_smem = (int)xysm;
+          c.z_smem = (int)zsm;
+          c.xy_blocks = (int)xy_blocks;
+          c.z_blocks = (int)z_blocks;
+          cand[pos] = c;
+          cscore[pos] = score;
+          if (ncand < max_out) ++ncand;
         }
       }
     }
   }
-  if (!found) {
+  if (ncand == 0) {
     if (why) *why = "no tiling of y=" + std::to_string(ny) + ", z=" + std::to_string(nz) +
                     " fits in shared memory with the supported radices";
-    return false;
+    return 0;
   }
-  P = best;
-  // 32-bit offsets address every real and spectral element
-  const long long spec = (long long)P.Ay * P.KG * P.nz * P.By * P.W;
-  if ((long long)nx * ny * nz >= (1ll << 31) || spec >= (1ll << 31)) {
-    if (why) *why = "work box of 2^31 voxels or more";
-    return false;
-  }
-  P.xy_threads = 256;
-  P.z_threads = 256;
-  P.spec_elems = (long long)P.Ay * P.KG * P.nz * P.By * P.W;
-  // twiddle buffer layout
-  int off = 0;
-  P.ax.tw_off = off; off += std::max(P.M, 1);
-  P.ayB.tw_off = off; off += std::max(P.By, 1);
-  P.az.tw_off = off; off += std::max(P.nz, 1);
-  P.tw_r2c_off = off; off += P.M / 2 + 1;
-  P.tw_ny_off = off; off += P.ny;
-  P.twiddle_count = off;
-  P.xrev_off = 0;
-  P.xrev_count = P.M;
-  *out = P;
-  return true;
+  int nout = 0;
+  for (int c = 0; c < ncand; ++c)
+    if (finalize_plan(cand[c], why)) out[nout++] = cand[c];
+  return nout;
 }
 
 

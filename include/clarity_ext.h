@@ -43,6 +43,25 @@ CLARITY_API ClarityResult_t clarityx_wiener_device(
 CLARITY_API ClarityResult_t clarityx_ml_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+/* Richardson-Lucy on `count` independent volumes of any sizes (device
+ * pointers, one kernel per volume): each volume has its own plan and
+ * workspace and the volumes run concurrently on a pool of streams, forked
+ * from and joined back to `stream`.  flags & CLARITYX_BATCH_GRAPH captures the
+ * whole batch into one CUDA graph, kept and replayed when the same batch
+ * (same pointers, sizes and iterations) is run again.  Asynchronous like the
+ * other _device calls.  Extension of Clarity_MaximumLikelihoodDeconvolve
+ * (Clarity.h.in:337-341), which takes one volume. */
+#define CLARITYX_BATCH_GRAPH 1
+CLARITY_API ClarityResult_t clarityx_ml_batch_device(
+    int count, const float *const *images, const Clarity_Dim3 *imageDims,
+    const float *const *kernels, const Clarity_Dim3 *kernelDims,
+    float *const *outs, int iterations, int flags, void *stream);
+
+/* Autotuning of work-box plans (off by default): with it on, the first use of
+ * a work box times the planner's best candidate tilings (one RL iteration's
+ * passes each) and keeps the fastest. */
+CLARITY_API void clarityx_autotune(int on);
+
 CLARITY_API ClarityResult_t clarityx_blind_ml_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);

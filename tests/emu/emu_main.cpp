@@ -49,6 +49,45 @@ int main(int argc, char** argv) {
     float* sig[3] = {&sx, &sy, &sz};
     r = Clarity_SmoothedJansenVanCittertDeconvolve(img.data(), id, psf.data(), kd, out.data(),
                                                    (unsigned)param, 2u, sig);
+  } else if (op == "batch") {
+    // three volumes of different sizes in one batched call (emulated device
+    // memory is host memory); each must equal its single-volume solve
+    const int n = 3;
+    Clarity_Dim3 bid[n] = {id, {id.x / 2 > 0 ? id.x / 2 : 1, id.y, id.z}, id};
+    {
+      int info[16];
+      const Clarity_Dim3 w1{bid[1].x + kd.x, bid[1].y + kd.y, bid[1].z + kd.z};
+      if (clarityx_plan_info(w1, info, 16) != CLARITY_SUCCESS) bid[1] = id;  // unsupported box
+    }
+    std::vector<float> vin[n], vout[n];
+    const float* ip[n];
+    const float* kp[n];
+    float* op_[n];
+    Clarity_Dim3 bkd[n] = {kd, kd, kd};
+    for (int v = 0; v < n; ++v) {
+      vin[v].resize((size_t)bid[v].x * bid[v].y * bid[v].z);
+      for (int z = 0; z < bid[v].z; ++z)
+        for (int y = 0; y < bid[v].y; ++y)
+          for (int x = 0; x < bid[v].x; ++x)
+            vin[v][((size_t)z * bid[v].y + y) * bid[v].x + x] =
+                img[((size_t)z * id.y + y) * id.x + x] * (1.0f + 0.25f * v);
+      vout[v].assign(vin[v].size(), -1.f);
+      ip[v] = vin[v].data();
+      kp[v] = psf.data();
+      op_[v] = vout[v].data();
+    }
+    r = clarityx_ml_batch_device(n, ip, bid, kp, bkd, op_, (int)param, CLARITYX_BATCH_GRAPH,
+                                 nullptr);
+    for (int v = 0; v < n && r == CLARITY_SUCCESS; ++v) {
+      std::vector<float> one(vin[v].size());
+      r = Clarity_MaximumLikelihoodDeconvolve(vin[v].data(), bid[v], psf.data(), kd, one.data(),
+                                              (int)param);
+      if (r == CLARITY_SUCCESS && std::memcmp(one.data(), vout[v].data(), 4 * one.size()) != 0) {
+        std::fprintf(stderr, "batch volume %d differs from its single solve\n", v);
+        return 5;
+      }
+    }
+    out = vout[0];
   } else if (op == "convolve_noalloc")  // emulated device memory is host memory
     r = clarityx_convolve_noalloc(img.data(), id, psf.data(), kd, out.data(), nullptr);
   else if (op == "wiener")

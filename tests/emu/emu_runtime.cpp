@@ -85,6 +85,15 @@ cudaError_t cudaEventRecord(cudaEvent_t e, cudaStream_t) {
   return cudaSuccess;
 }
 cudaError_t cudaEventSynchronize(cudaEvent_t) { return cudaSuccess; }
+cudaError_t cudaEventCreateWithFlags(cudaEvent_t* e, unsigned int) { return cudaEventCreate(e); }
+cudaError_t cudaEventDestroy(cudaEvent_t e) {
+  delete reinterpret_cast<double*>(e);
+  return cudaSuccess;
+}
+// the emulation never instantiates graphs (batches run as issued)
+cudaError_t cudaGraphExecDestroy(cudaGraphExec_t) { return cudaSuccess; }
+// every emulated kernel has finished when its launch returns: waits are no-ops
+cudaError_t cudaStreamWaitEvent(cudaStream_t, cudaEvent_t, unsigned int) { return cudaSuccess; }
 cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t a, cudaEvent_t b) {
   *ms = (float)(*reinterpret_cast<double*>(b) - *reinterpret_cast<double*>(a));
   return cudaSuccess;

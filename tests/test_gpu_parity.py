@@ -175,3 +175,61 @@ def test_device_api_matches_host_api(clarity_gpu):
     torch.cuda.synchronize()
     host = clarity_gpu.maximum_likelihood_deconvolve(d["image"], d["psf"], 5)
     assert np.array_equal(out.cpu().numpy(), host)
+
+
+def _batch_inputs(seed, shapes):
+    r = syn.rng(seed)
+    imgs, psfs = [], []
+    for sh in shapes:
+        imgs.append((r.random(sh) * 100 + 1).astype(np.float32))
+        psfs.append(syn.gaussian_psf(sh, 1.2, 1.5).astype(np.float32))
+    return imgs, psfs
+
+
+def test_batched_rl_uneven_volumes(clarity_gpu, oracle_lib):
+    # configs[2] form at small sizes: volumes of uneven sizes in one call, run
+    # directly and as a captured CUDA graph (captured, then replayed)
+    import torch
+    shapes = [(8, 24, 16), (12, 20, 28), (16, 32, 32), (6, 18, 22), (10, 16, 24)]
+    imgs, psfs = _batch_inputs(11, shapes)
+    di = [torch.from_numpy(a).cuda() for a in imgs]
+    dk = [torch.from_numpy(a).cuda() for a in psfs]
+    direct = [torch.full_like(a, -1.0) for a in di]
+    clarity_gpu.ml_batch_device(di, dk, direct, 4, graph=False)
+    torch.cuda.synchronize()
+    for img, psf, out in zip(imgs, psfs, direct):
+        assert rel_l2(out.cpu().numpy(), oracle_lib.rl(img, psf, 4)) <= TOL_ITER
+    for _ in range(2):  # capture + launch, then replay
+        graphed = [torch.full_like(a, -1.0) for a in di]
+        clarity_gpu.ml_batch_device(di, dk, graphed, 4, graph=True)
+        torch.cuda.synchronize()
+        for a, b in zip(direct, graphed):
+            assert torch.equal(a, b)
+    # a batched volume equals its single-volume solve
+    one = torch.empty_like(di[1])
+    clarity_gpu.ml_device(di[1], dk[1], one, 4)
+    torch.cuda.synchronize()
+    assert torch.equal(one, direct[1])
+
+
+def test_batch_argument_errors(clarity_gpu):
+    import torch
+    a = torch.ones((4, 4, 4), device="cuda")
+    empty = torch.ones((0, 4, 4), device="cuda")
+    out = torch.empty_like(a)
+    with pytest.raises(clarity_gpu.ClarityError) as e:
+        clarity_gpu.ml_batch_device([a, empty], [a, a], [out, out], 2)
+    assert e.value.code == clarity_gpu.CLARITY_INVALID_ARGUMENT
+    assert "dimension" in str(e.value)
+    clarity_gpu.ml_batch_device([], [], [], 3)  # empty batch is a no-op
+
+
+def test_autotuned_plan_matches_oracle(clarity_gpu, oracle_lib):
+    # the autotuner may pick any candidate tiling: results stay within parity
+    img, psf = _batch_inputs(12, [(12, 40, 36)])
+    clarity_gpu.autotune(True)
+    try:
+        out = clarity_gpu.maximum_likelihood_deconvolve(img[0], psf[0], 3)
+    finally:
+        clarity_gpu.autotune(False)
+    assert rel_l2(out, oracle_lib.rl(img[0], psf[0], 3)) <= TOL_ITER
