@@ -56,6 +56,7 @@ EXTENSION_SYMBOLS = [
     "clarityx_jvc_device", "clarityx_idivergence", "clarityx_plan_info",
     "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
     "clarityx_convolve_noalloc", "clarityx_ml_batch_device", "clarityx_autotune",
+    "clarityx_ml_ex_device", "clarityx_ml_accel_device",
 ]
 BATCH_GRAPH = 1  # CLARITYX_BATCH_GRAPH
 
@@ -142,6 +143,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                                C.POINTER(vp), C.POINTER(Dim3),
                                                C.POINTER(vp), i, i, vp]
         L.clarityx_ml_batch_device.restype = i
+        L.clarityx_ml_ex_device.argtypes = [vp, Dim3, vp, Dim3, vp, vp, i, vp, vp]
+        L.clarityx_ml_ex_device.restype = i
+        L.clarityx_ml_accel_device.argtypes = [vp, Dim3, vp, Dim3, vp, i, vp, vp]
+        L.clarityx_ml_accel_device.restype = i
         L.clarityx_autotune.argtypes = [i]
         L.clarityx_autotune.restype = None
         L.clarityx_launch_count.restype = C.c_longlong
@@ -384,3 +389,42 @@ def ml_batch_device(images, kernels, outs, iterations, graph=True, stream=None):
 def autotune(on: bool = True) -> None:
     """clarityx_autotune: time candidate plans on first use of a work box."""
     load().clarityx_autotune(1 if on else 0)
+
+
+def ml_ex_device(image, kernel, out, iterations, start=None, idiv=None, stream=None):
+    """clarityx_ml_ex_device: RL from `start` (an image-shaped device tensor;
+    None: the image) with an optional I-divergence trace into `idiv` (a float64
+    device tensor of `iterations` + 1 entries: the estimate at the start of each
+    iteration, then the result)."""
+    for t in (image, kernel, out) + ((start,) if start is not None else ()):
+        if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+            raise ValueError("device variants need contiguous float32 CUDA tensors")
+    if start is not None and tuple(start.shape) != tuple(image.shape):
+        raise ValueError("start must have the image's shape")
+    if idiv is not None and not (idiv.is_cuda and str(idiv.dtype) == "torch.float64"
+                                 and idiv.numel() >= max(int(iterations), 0) + 1):
+        raise ValueError("idiv must be a float64 CUDA tensor of `iterations` + 1 entries")
+    vp = C.c_void_p
+    _check(load().clarityx_ml_ex_device(
+        vp(image.data_ptr()), dim3(image), vp(kernel.data_ptr()), dim3(kernel),
+        vp(start.data_ptr()) if start is not None else None, vp(out.data_ptr()),
+        int(iterations), vp(idiv.data_ptr()) if idiv is not None else None,
+        _stream_ptr(stream)))
+    return out
+
+
+def ml_accel_device(image, kernel, out, iterations, idiv=None, stream=None):
+    """clarityx_ml_accel_device: accelerated RL (Biggs-Andrews extrapolation)
+    with an optional I-divergence trace (`iterations` + 1 float64 entries)."""
+    for t in (image, kernel, out):
+        if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+            raise ValueError("device variants need contiguous float32 CUDA tensors")
+    if idiv is not None and not (idiv.is_cuda and str(idiv.dtype) == "torch.float64"
+                                 and idiv.numel() >= max(int(iterations), 0) + 1):
+        raise ValueError("idiv must be a float64 CUDA tensor of `iterations` + 1 entries")
+    vp = C.c_void_p
+    _check(load().clarityx_ml_accel_device(
+        vp(image.data_ptr()), dim3(image), vp(kernel.data_ptr()), dim3(kernel),
+        vp(out.data_ptr()), int(iterations), vp(idiv.data_ptr()) if idiv is not None else None,
+        _stream_ptr(stream)))
+    return out

@@ -96,7 +96,7 @@ ClarityResult_t host_call(const float* in, Clarity_Dim3 id, const float* ker,
   if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
-  ctx->set_stream(nullptr);
+  ctx->clear_stream();
   const size_t ni = (size_t)nvox(id), nk = (size_t)nvox(kd);
   Status s = grow(&g_stage.img, &g_stage.img_cap, ni);
   if (s.ok()) s = grow(&g_stage.ker, &g_stage.ker_cap, nk);
@@ -133,7 +133,7 @@ ClarityResult_t device_call(const float* in, Clarity_Dim3 id, const float* ker,
   cudaSetDevice(ctx->device());
   ctx->set_stream(static_cast<cudaStream_t>(stream));
   Status s = run(*ctx, in, to_dims(id), ker, to_dims(kd), out);
-  ctx->set_stream(nullptr);
+  ctx->clear_stream();
   return report(s);
 }
 
@@ -408,6 +408,27 @@ ClarityResult_t clarityx_ml_device(const float* image, Clarity_Dim3 imageDim,
                      });
 }
 
+ClarityResult_t clarityx_ml_ex_device(const float* image, Clarity_Dim3 imageDim,
+                                      const float* kernel, Clarity_Dim3 kernelDim,
+                                      const float* start, float* out, int iterations,
+                                      double* idiv, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_rl_ex(c, i, id, k, kd, start, o, iterations, idiv);
+                     });
+}
+
+ClarityResult_t clarityx_ml_accel_device(const float* image, Clarity_Dim3 imageDim,
+                                         const float* kernel, Clarity_Dim3 kernelDim, float* out,
+                                         int iterations, double* idiv, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_rl_accel(c, i, id, k, kd, o, iterations, idiv);
+                     });
+}
+
 ClarityResult_t clarityx_ml_batch_device(int count, const float* const* images,
                                          const Clarity_Dim3* imageDims,
                                          const float* const* kernels,
@@ -435,7 +456,7 @@ ClarityResult_t clarityx_ml_batch_device(int count, const float* const* images,
   ctx->set_stream(static_cast<cudaStream_t>(stream));
   Status s = clarity::run_rl_batch(*ctx, count, images, ids.data(), kernels, kds.data(), outs,
                                    iterations, (flags & CLARITYX_BATCH_GRAPH) != 0);
-  ctx->set_stream(nullptr);
+  ctx->clear_stream();
   return report(s);
 }
 
@@ -477,7 +498,7 @@ ClarityResult_t clarityx_idivergence(const float* g, const float* ghat, long lon
   if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
-  ctx->set_stream(nullptr);
+  ctx->clear_stream();
   float *dg = nullptr, *dh = nullptr;
   cudaError_t e = clarity::dev_alloc((void**)&dg, sizeof(float) * n);
   if (e == cudaSuccess) e = clarity::dev_alloc((void**)&dh, sizeof(float) * n);

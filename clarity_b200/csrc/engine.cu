@@ -115,6 +115,21 @@ int static_family_mask() {
 
 static inline void count_small() { g_launches.fetch_add(1); }
 
+cudaError_t smem_opt_in(const void* kernel, int smem) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;  // (kernel, device) -> bytes
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  int& have = done[{kernel, dev}];
+  if (have >= smem) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) have = smem;
+  return e;
+}
+
 bool xy_tma_enabled() {
   static const bool on = [] {
     const char* v = std::getenv("CLARITY_XY_TMA");
@@ -221,6 +236,63 @@ __device__ __forceinline__ double block_total(const double* partial, int np) {
 // sum -> dout[0]
 __global__ void k_finish_sum(const double* partial, int np, double* dout) {
   const double t = block_total(partial, np);
+  if (threadIdx.x == 0) dout[0] = t;
+}
+
+// The image on the work box (zero padding), as the first RL estimate.
+__global__ void k_pad_image(ImageSrc g, WorkVol w, float* __restrict__ out) {
+  const long long n = (long long)w.nx * w.ny * w.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % w.nx);
+    const long long r = i / w.nx;
+    out[i] = g.at(x, (int)(r % w.ny), (int)(r / w.ny));
+  }
+}
+
+// Accelerated RL step bookkeeping: x_next = s u' (in place over u'),
+// g_k = x_next - y, and (after the first step) FP64 sums of g_k g_{k-1} and
+// g_{k-1}^2 per block into partial[2b], partial[2b+1]; g_{k-1} is replaced by
+// g_k.
+__global__ void k_accel_update(float* __restrict__ u, const float* __restrict__ y,
+                               float* __restrict__ gprev, const float* __restrict__ scale,
+                               int first, long long n, double* __restrict__ partial) {
+  const float s = *scale;
+  double d1 = 0, d2 = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = s * u[i];
+    const float g = v - y[i];
+    if (!first) {
+      const float gp = gprev[i];
+      d1 += (double)g * (double)gp;
+      d2 += (double)gp * (double)gp;
+    }
+    gprev[i] = g;
+    u[i] = v;
+  }
+  block_sum_store(d1, partial + 0 * gridDim.x);
+  block_sum_store(d2, partial + 1 * gridDim.x);
+}
+
+// alpha = sum(g_k g_{k-1}) / sum(g_{k-1}^2) clamped to [0, 1], as float.
+__global__ void k_finish_alpha(const double* partial, int np, float* alpha) {
+  const double a = block_total(partial, np);
+  __syncthreads();
+  const double b = block_total(partial + np, np);
+  if (threadIdx.x == 0) {
+    float r = 0.f;
+    if (b > 0) {
+      r = (float)(a / b);
+      r = r < 0.f ? 0.f : (r > 1.f ? 1.f : r);
+    }
+    *alpha = r;
+  }
+}
+
+// sum of *np partials -> *dout (the count is written by the producing pass)
+__global__ void k_finish_sum_np(const double* partial, const int* np, double* dout) {
+  const double t = block_total(partial, *np);
   if (threadIdx.x == 0) dout[0] = t;
 }
 
@@ -340,6 +412,7 @@ static void free_workspace(Workspace& w) {
   cudaFree(w.S); cudaFree(w.H); cudaFree(w.u); cudaFree(w.img); cudaFree(w.ker);
   cudaFree(w.partial); cudaFree(w.dscal); cudaFree(w.fscal); cudaFree(w.iscal);
   cudaFree(w.HG);
+  for (float* b : w.accel) cudaFree(b);
   w = Workspace();
 }
 
@@ -702,21 +775,38 @@ Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
 // then s = E / sum(u') on the device.  cur = s*u' is never stored: P5 reads
 // u' and s, and P2 of the next iteration applies s to the transform of u'
 // (the flux rescale of :73-78, deferred).
+// start: the first estimate (an image-sized volume, zero in the padding;
+// nullptr: the image itself, as the reference).  idiv: when not null,
+// idiv[k] (k < iters) receives the I-divergence of the image against
+// h * (estimate at the start of iteration k), accumulated by the ratio pass,
+// and idiv[iters] that of the result.
 static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
                       const float* img, Dims id, Dims wd, int iters,
-                      bool rescale) {
+                      bool rescale, const float* start = nullptr, double* idiv = nullptr) {
   const VolPlan& P = pe.P;
   cudaStream_t st = ctx.exec_stream();
   const ImageSrc g = image_src(img, id);
+  const ImageSrc u0 = start ? image_src(start, id) : g;
   const WorkVol wv{wd.x, wd.y, wd.z};
   const float scale_n = inv_volume(wd);
   float* sdev = ws.fscal;  // deferred flux scale
   if (rescale) CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
-  CL_TRY(xy_forward(ctx, pe, ProImage{g, P.xmode}, ws.S));
+  CL_TRY(xy_forward(ctx, pe, ProImage{u0, P.xmode}, ws.S));
   for (int k = 0; k < iters; ++k) {
     const float* sk = (k == 0 || !rescale) ? nullptr : sdev;
     CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n, sk}, ws.S, ws.S));
-    CL_TRY(xy_inv_fwd(ctx, pe, MidRLRatio{g, P.xmode}, ws.S));
+    MidRLRatio ratio{g, P.xmode};
+    if (idiv) {
+      ratio.idiv_partial = ws.partial;
+      ratio.nblocks = ws.iscal + 1;
+    }
+    CL_TRY(xy_inv_fwd(ctx, pe, ratio, ws.S));
+    if (idiv) {
+      // read before the product pass reuses the partials
+      count_small();
+      CLARITY_LAUNCH(k_finish_sum_np, 1, 256, 0, st)(ws.partial, ws.iscal + 1, idiv + k);
+      CL_CHECK(cudaGetLastError());
+    }
     // the ratio is zero in planes z >= Z (the image is zero there): P3 does
     // not write them and this pass reads them as zeros
     ModOTF m4{ws.H, scale_n};
@@ -724,7 +814,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     CL_TRY(z_pass(ctx, pe, m4, ws.S, ws.S));
     EpiRLProduct epi;
     epi.cur = (k == 0) ? nullptr : ws.u;
-    epi.g = g;
+    epi.g = u0;
     epi.scale = sk;
     epi.unew = ws.u;
     epi.partial = ws.partial;
@@ -743,13 +833,27 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
       CL_CHECK(cudaGetLastError());
     }
   }
+  if (idiv && iters > 0) {
+    // idiv[iters]: the result's own I-divergence (h * s u', one more forward
+    // transform, z pass and xy inverse that only accumulates)
+    CL_TRY(xy_forward(ctx, pe, ProWork{ws.u, rescale ? sdev : nullptr, wv, P.xmode}, ws.S));
+    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n}, ws.S, ws.S));
+    MidRLRatio tr{g, P.xmode};
+    tr.idiv_partial = ws.partial;
+    tr.nblocks = ws.iscal + 1;
+    CL_TRY(xy_inverse(ctx, pe, tr, ws.S));
+    count_small();
+    CLARITY_LAUNCH(k_finish_sum_np, 1, 256, 0, st)(ws.partial, ws.iscal + 1, idiv + iters);
+    CL_CHECK(cudaGetLastError());
+  }
   return Status::Ok();
 }
 
 // One Richardson-Lucy solve on prepared plan and workspace, enqueued on
 // ctx.exec_stream(): OTF, the iterations, the clipped result.
 static Status rl_solve(Context& ctx, const PlanEntry& pe, Workspace& ws, const float* img,
-                       Dims id, const float* ker, Dims kd, Dims wd, float* out, int iters) {
+                       Dims id, const float* ker, Dims kd, Dims wd, float* out, int iters,
+                       const float* start = nullptr, double* idiv = nullptr) {
   cudaStream_t st = ctx.exec_stream();
   if (iters <= 0) {
     // the reference leaves the output unwritten; return the input image
@@ -759,7 +863,7 @@ static Status rl_solve(Context& ctx, const PlanEntry& pe, Workspace& ws, const f
     return Status::Ok();
   }
   CL_TRY(make_otf(ctx, pe, ker, kd, wd, ws.H, nullptr));
-  CL_TRY(rl_core(ctx, pe, ws, img, id, wd, iters, true));
+  CL_TRY(rl_core(ctx, pe, ws, img, id, wd, iters, true, start, idiv));
   count_small();
   CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws.u, wd.x, wd.y, out, id.x, id.y, id.z,
                                                     ws.fscal);
@@ -770,9 +874,16 @@ static Status rl_solve(Context& ctx, const PlanEntry& pe, Workspace& ws, const f
 // Runs a scope's enqueues on another stream of the context.
 struct StreamScope {
   Context& ctx;
+  bool had;
   cudaStream_t saved;
-  StreamScope(Context& c, cudaStream_t s) : ctx(c), saved(c.user_stream()) { c.set_stream(s); }
-  ~StreamScope() { ctx.set_stream(saved); }
+  StreamScope(Context& c, cudaStream_t s)
+      : ctx(c), had(c.has_user_stream()), saved(c.exec_stream()) {
+    c.set_stream(s);
+  }
+  ~StreamScope() {
+    if (had) ctx.set_stream(saved);
+    else ctx.clear_stream();
+  }
 };
 
 Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
@@ -782,6 +893,137 @@ Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
   Dims wd;
   CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
   return rl_solve(ctx, *pe, *ws, img, id, ker, kd, wd, out, iters);
+}
+
+Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                 const float* start, float* out, int iters, double* idiv) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  if (iters <= 0 && start) {
+    count_small();
+    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, ctx.exec_stream())(start, out, id.n());
+    CL_CHECK(cudaGetLastError());
+    return Status::Ok();
+  }
+  return rl_solve(ctx, *pe, *ws, img, id, ker, kd, wd, out, iters, start, idiv);
+}
+
+// Accelerated Richardson-Lucy (Biggs and Andrews, Applied Optics
+// 36(8):1766-1775, 1997; no reference counterpart).  Per iteration:
+//   P1 xy forward of y = max(0, x + alpha (x - x_prev)), y stored (ProAccel)
+//   P2-P4 as plain RL (z, ratio, z) -- the ratio pass may trace I-div at y
+//   P5 xy inverse, u' = y * (h*r), FP64 sums -> s = E / sum u'
+//   x_next = s u', g_k = x_next - y, sums of g_k g_{k-1}, g_{k-1}^2 -> alpha
+// The three estimate buffers rotate (x_prev, x, x_next); idiv as run_rl_ex,
+// its entries k < iters taken at y_k.
+Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                    float* out, int iters, double* idiv) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  cudaStream_t st = ctx.exec_stream();
+  if (iters <= 0) {
+    count_small();
+    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, st)(img, out, id.n());
+    CL_CHECK(cudaGetLastError());
+    return Status::Ok();
+  }
+  const VolPlan& P = pe->P;
+  const long long n = wd.n();
+  if (ws->accel_cap < n) {
+    for (float*& b : ws->accel) {
+      cudaFree(b);
+      b = nullptr;
+    }
+    ws->accel_cap = 0;
+    for (float*& b : ws->accel) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
+    ws->accel_cap = n;
+  }
+  // partials: one per XY block for the flux sum, two per reduce block for
+  // the extrapolation sums
+  {
+    long long pc = ws->partial_cap;
+    CL_TRY(ensure(&ws->partial, &pc, 2 * (long long)kReduceBlocks));
+    ws->partial_cap = (int)pc;
+  }
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  const ImageSrc g = image_src(img, id);
+  const WorkVol wv{wd.x, wd.y, wd.z};
+  const float scale_n = inv_volume(wd);
+  float* B[3] = {ws->accel[0], ws->accel[1], ws->accel[2]};
+  float* Y = ws->accel[3];
+  float* G = ws->accel[4];
+  float* alpha = ws->fscal + 6;
+  float* sdev = ws->fscal;
+  int xi = 0, pi = 0, ui = 1;  // x, x_prev, x_next buffers (x_prev = x at first)
+  CL_TRY(reduce_sum_into(ctx, img, id.n(), ws->partial, ws->dscal + 0));
+  count_small();
+  CLARITY_LAUNCH(k_pad_image, kReduceBlocks, 256, 0, st)(g, wv, B[0]);
+  CL_CHECK(cudaMemsetAsync(alpha, 0, sizeof(float), st));
+  for (int k = 0; k < iters; ++k) {
+    CL_TRY(xy_forward(ctx, *pe, ProAccel{B[xi], B[pi], alpha, Y, wv, P.xmode}, ws->S));
+    CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, scale_n}, ws->S, ws->S));
+    MidRLRatio ratio{g, P.xmode};
+    if (idiv) {
+      ratio.idiv_partial = ws->partial;
+      ratio.nblocks = ws->iscal + 1;
+    }
+    CL_TRY(xy_inv_fwd(ctx, *pe, ratio, ws->S));
+    if (idiv) {
+      count_small();
+      CLARITY_LAUNCH(k_finish_sum_np, 1, 256, 0, st)(ws->partial, ws->iscal + 1, idiv + k);
+      CL_CHECK(cudaGetLastError());
+    }
+    ModOTF m4{ws->H, scale_n};
+    m4.zn = id.z;
+    CL_TRY(z_pass(ctx, *pe, m4, ws->S, ws->S));
+    EpiRLProduct epi;
+    epi.cur = Y;
+    epi.g = g;
+    epi.scale = nullptr;
+    epi.unew = B[ui];
+    epi.partial = ws->partial;
+    epi.w = wv;
+    epi.xmode = P.xmode;
+    epi.acc = 0.0;
+    epi.nblocks = ws->iscal;
+    CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
+    count_small();
+    CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws->partial, ws->iscal, ws->dscal + 0,
+                                                     ws->dscal + 1, sdev);
+    count_small();
+    CLARITY_LAUNCH(k_accel_update, kReduceBlocks, 256, 0, st)(B[ui], Y, G, sdev, k == 0 ? 1 : 0,
+                                                              n, ws->partial);
+    CL_CHECK(cudaGetLastError());
+    if (k > 0) {
+      count_small();
+      CLARITY_LAUNCH(k_finish_alpha, 1, 256, 0, st)(ws->partial, kReduceBlocks, alpha);
+      CL_CHECK(cudaGetLastError());
+    }
+    // rotate: x_prev <- x, x <- x_next, x_next <- the free buffer
+    pi = xi;
+    xi = ui;
+    ui = 3 - pi - xi;
+  }
+  if (idiv) {
+    CL_TRY(xy_forward(ctx, *pe, ProWork{B[xi], nullptr, wv, P.xmode}, ws->S));
+    CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, scale_n}, ws->S, ws->S));
+    MidRLRatio tr{g, P.xmode};
+    tr.idiv_partial = ws->partial;
+    tr.nblocks = ws->iscal + 1;
+    CL_TRY(xy_inverse(ctx, *pe, tr, ws->S));
+    count_small();
+    CLARITY_LAUNCH(k_finish_sum_np, 1, 256, 0, st)(ws->partial, ws->iscal + 1, idiv + iters);
+    CL_CHECK(cudaGetLastError());
+  }
+  count_small();
+  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(B[xi], wd.x, wd.y, out, id.x, id.y, id.z,
+                                                    nullptr);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
 }
 
 // Batched Richardson-Lucy.  Set-up (plans, possibly autotuned, and one
@@ -814,11 +1056,14 @@ Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* i
     CL_TRY(ctx.workspace_slot(i, *pes[i], ids[i], kds[i], &wss[i]));
   }
   for (int j = 0; j < ns; ++j) CL_TRY(ctx.batch_stream(j, &bs[j]));
-  const cudaStream_t origin = ctx.exec_stream();
+  // the caller's stream; a graph is captured on and launched from the
+  // context's own stream (capture is not allowed on the legacy default
+  // stream), ordered after and before the caller's work by events
+  const cudaStream_t caller = ctx.exec_stream();
+  const cudaStream_t origin = use_graph ? ctx.own_stream() : caller;
   std::vector<unsigned long long> key;
   key.push_back((unsigned long long)n);
   key.push_back((unsigned long long)iters);
-  key.push_back((unsigned long long)(uintptr_t)origin);
   for (int i = 0; i < n; ++i) {
     for (const void* p : {(const void*)imgs[i], (const void*)kers[i], (const void*)outs[i],
                           (const void*)wss[i]->S, (const void*)wss[i]->H,
@@ -829,10 +1074,30 @@ Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* i
     key.push_back(((unsigned long long)kds[i].x << 42) | ((unsigned long long)kds[i].y << 21) |
                   (unsigned long long)kds[i].z);
   }
+  // caller -> origin -> caller ordering around a graph launch
+  auto after_caller = [&]() -> Status {
+    cudaEvent_t e = nullptr;
+    CL_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaError_t r = cudaEventRecord(e, caller);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(origin, e, 0);
+    cudaEventDestroy(e);
+    CL_CHECK(r);
+    return Status::Ok();
+  };
+  auto before_caller = [&]() -> Status {
+    cudaEvent_t e = nullptr;
+    CL_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaError_t r = cudaEventRecord(e, origin);
+    if (r == cudaSuccess) r = cudaStreamWaitEvent(caller, e, 0);
+    cudaEventDestroy(e);
+    CL_CHECK(r);
+    return Status::Ok();
+  };
   if (use_graph) {
     if (cudaGraphExec_t g = ctx.find_graph(key)) {
+      CL_TRY(after_caller());
       CL_CHECK(cudaGraphLaunch(g, origin));
-      return Status::Ok();
+      return before_caller();
     }
   }
   auto issue = [&]() -> Status {
@@ -880,7 +1145,9 @@ Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* i
   cudaGraphDestroy(graph);
   CL_CHECK(ie);
   ctx.add_graph(std::move(key), exec);
+  CL_TRY(after_caller());
   CL_CHECK(cudaGraphLaunch(exec, origin));
+  CL_TRY(before_caller());
 #endif
   return Status::Ok();
 }

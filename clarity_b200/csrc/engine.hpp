@@ -57,6 +57,8 @@ struct Workspace {
   double* dscal = nullptr; // [0] energy, [1] last sum, [2..] misc
   float* fscal = nullptr;  // [0] deferred scale, [1] ones, [2..] misc
   int* iscal = nullptr;    // [0] number of partial sums the last product pass wrote
+  float* accel[5] = {};    // accelerated RL: three estimates, extrapolated point, step
+  long long accel_cap = 0;
   size_t img_cap = 0, ker_cap = 0;
   long long spec_cap = 0, work_cap = 0;
   int partial_cap = 0;
@@ -68,9 +70,14 @@ class Context {
   ~Context();
   int device() const { return device_; }
   cudaStream_t stream() const { return stream_; }
-  void set_stream(cudaStream_t s) { user_stream_ = s; }
-  cudaStream_t user_stream() const { return user_stream_; }
-  cudaStream_t exec_stream() const { return user_stream_ ? user_stream_ : stream_; }
+  // The stream work is enqueued on: the caller's (any handle, 0 included,
+  // which is the legacy default stream) while one is set, else the context's
+  // own stream (the synchronous host API).
+  void set_stream(cudaStream_t s) { user_stream_ = s; has_user_stream_ = true; }
+  void clear_stream() { user_stream_ = nullptr; has_user_stream_ = false; }
+  cudaStream_t exec_stream() const { return has_user_stream_ ? user_stream_ : stream_; }
+  cudaStream_t own_stream() const { return stream_; }
+  bool has_user_stream() const { return has_user_stream_; }
 
   Status plan(const Dims& work, const PlanEntry** out);
   Status workspace(const PlanEntry& pe, const Dims& img, const Dims& ker,
@@ -98,6 +105,7 @@ class Context {
   int device_;
   cudaStream_t stream_ = nullptr;
   cudaStream_t user_stream_ = nullptr;
+  bool has_user_stream_ = false;
   Status build_entry(const VolPlan& P, std::unique_ptr<PlanEntry>* out);
   Status tune(const Dims& wd, std::unique_ptr<PlanEntry>* out);
   std::map<std::tuple<int, int, int>, std::unique_ptr<PlanEntry>> plans_;
@@ -121,6 +129,16 @@ Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
                   Dims kd, float* out, float eps);
 Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
               Dims kd, float* out, int iters);
+// Richardson-Lucy from a given first estimate (image-sized, nullptr: the
+// image) with an optional I-divergence trace idiv[0..iters) (device doubles:
+// the image against h * the estimate at the start of each iteration).
+Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                 const float* start, float* out, int iters, double* idiv);
+// Accelerated Richardson-Lucy (Biggs-Andrews vector extrapolation), optional
+// I-divergence trace as run_rl_ex (entries k < iters at the extrapolated
+// points).
+Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                    float* out, int iters, double* idiv);
 // Richardson-Lucy on n independent volumes of any sizes (device pointers):
 // each volume has its own plan and workspace, volumes run concurrently on the
 // batch stream pool, and with use_graph the whole batch is captured into one
@@ -147,6 +165,10 @@ void set_last_error(const char* msg);
 void note_launch_begin(int kind, cudaStream_t st);
 void note_launch_end(int kind, cudaStream_t st);
 void set_capturing(bool on);
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) for kernels above 48 KB,
+// issued once per kernel, device and size (the attribute call is not free, and
+// a solve launches each kernel hundreds of times).
+cudaError_t smem_opt_in(const void* kernel, int smem);
 long long launch_count();
 int static_family_mask();
 void timing_enable(bool on);

@@ -5,5 +5,6 @@ namespace clarity {
 template bool static_xy_inverse<EpiClip>(const PlanEntry&, cudaStream_t, const EpiClip&, const float2*, cudaError_t*);
 template bool static_xy_inverse<EpiWork>(const PlanEntry&, cudaStream_t, const EpiWork&, const float2*, cudaError_t*);
 template bool static_xy_inverse<EpiRLProduct>(const PlanEntry&, cudaStream_t, const EpiRLProduct&, const float2*, cudaError_t*);
+template bool static_xy_inverse<MidRLRatio>(const PlanEntry&, cudaStream_t, const MidRLRatio&, const float2*, cudaError_t*);
 template bool static_xy_inverse<EpiJVC>(const PlanEntry&, cudaStream_t, const EpiJVC&, const float2*, cudaError_t*);
 }  // namespace clarity

@@ -5,4 +5,5 @@ namespace clarity {
 template Status xy_forward<ProWork>(Context&, const PlanEntry&, const ProWork&, float2*);
 template Status xy_forward<ProPadded>(Context&, const PlanEntry&, const ProPadded&, float2*);
 template Status xy_forward<ProImage>(Context&, const PlanEntry&, const ProImage&, float2*);
+template Status xy_forward<ProAccel>(Context&, const PlanEntry&, const ProAccel&, float2*);
 }  // namespace clarity

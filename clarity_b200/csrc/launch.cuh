@@ -30,11 +30,8 @@ bool static_xy_inverse(const PlanEntry&, cudaStream_t, const F&, const float2*, 
 
 template <class K>
 static cudaError_t prep_kernel(K kernel, int smem) {
-  // Opt in to the dynamic shared memory this launch needs (idempotent).
-  if (smem > 48 * 1024)
-    return cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  return cudaSuccess;
+  // Opt in to the dynamic shared memory this launch needs (once per kernel).
+  return smem_opt_in(reinterpret_cast<const void*>(kernel), smem);
 }
 
 template <class Pro>
@@ -113,6 +110,8 @@ Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
                                                const ProPadded&, float2*);          \
   extern template Status xy_forward<ProImage>(Context&, const PlanEntry&,           \
                                               const ProImage&, float2*);            \
+  extern template Status xy_forward<ProAccel>(Context&, const PlanEntry&,           \
+                                              const ProAccel&, float2*);            \
   extern template Status xy_inverse<EpiClip>(Context&, const PlanEntry&,            \
                                              const EpiClip&, const float2*);        \
   extern template Status xy_inverse<EpiWork>(Context&, const PlanEntry&,            \
@@ -121,6 +120,8 @@ Status z_pass(Context& ctx, const PlanEntry& pe, const Mod& mod,
                                                   const EpiRLProduct&, const float2*); \
   extern template Status xy_inverse<EpiJVC>(Context&, const PlanEntry&,             \
                                             const EpiJVC&, const float2*);          \
+  extern template Status xy_inverse<MidRLRatio>(Context&, const PlanEntry&,         \
+                                                const MidRLRatio&, const float2*);  \
   extern template Status xy_inv_fwd<MidRLRatio>(Context&, const PlanEntry&,         \
                                                 const MidRLRatio&, float2*);        \
   extern template Status xy_inv_fwd<EpiJVC>(Context&, const PlanEntry&,             \

@@ -97,6 +97,37 @@ struct ProWork {
   __device__ __forceinline__ void finish() const {}
 };
 
+// Extrapolated estimate of accelerated RL (Biggs-Andrews): y = max(0,
+// x + alpha (x - xp)), one fused multiply-add, stored to yout on the way into
+// the forward transform (the product step reads it back as the estimate).
+struct ProAccel {
+  const float* __restrict__ x;
+  const float* __restrict__ xp;
+  const float* __restrict__ alpha;
+  float* __restrict__ yout;
+  WorkVol w;
+  int xmode;
+  __device__ __forceinline__ static float extrap(float a, float x, float xp) {
+    return fmaxf(0.f, fmaf(a, x - xp, x));
+  }
+  __device__ __forceinline__ float2 load_c(int m, int y, int z) const {
+    const float a = __ldg(alpha);
+    if (xmode == 0) {
+      const unsigned i = w.idx(2 * m, y, z);
+      const float2 xv = __ldg(reinterpret_cast<const float2*>(x + i));
+      const float2 pv = __ldg(reinterpret_cast<const float2*>(xp + i));
+      const float2 r = make_float2(extrap(a, xv.x, pv.x), extrap(a, xv.y, pv.y));
+      *reinterpret_cast<float2*>(yout + i) = r;
+      return r;
+    }
+    const unsigned i = w.idx(m, y, z);
+    const float r = extrap(a, __ldg(x + i), __ldg(xp + i));
+    yout[i] = r;
+    return make_float2(r, 0.f);
+  }
+  __device__ __forceinline__ void finish() const {}
+};
+
 // Unpadded source read through the pad/shift map, times an optional scale.
 struct ProPadded {
   PaddedSrc p;
@@ -284,7 +315,33 @@ struct MidRLRatio {
   static constexpr bool has_zero_rows = true;
   ImageSrc g;
   int xmode;
+  // Optional trace (idiv_partial != nullptr): the I-divergence of g against
+  // b = h*cur over the image, g ln(g/b) + b - g with 0 ln 0 = 0 (terms with
+  // g > 0 >= b skipped), summed in FP64 per block; block 0 stores the grid
+  // size in *nblocks.  Same definition as k_idiv and the oracle
+  // (IDIVFunctional, src/IDivergenceDeconvolve.cxx:33-47, alpha = 0).
+  double* __restrict__ idiv_partial = nullptr;
+  int* nblocks = nullptr;
+  double acc = 0.0;
+  __device__ __forceinline__ void idiv_add(float a, float b) {
+    if (a > 0.f) {
+      if (b > 0.f) {
+        const double da = a, db = b;
+        acc += da * log(da / db) + db - da;
+      }
+    } else {
+      acc += (double)b - (double)a;
+    }
+  }
   __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 b) {
+    if (idiv_partial && y < g.Y && z < g.Z) {
+      if (xmode == 0) {
+        if (2 * m < g.X) idiv_add(g.at(2 * m, y, z), b.x);
+        if (2 * m + 1 < g.X) idiv_add(g.at(2 * m + 1, y, z), b.y);
+      } else if (m < g.X) {
+        idiv_add(g.at(m, y, z), b.x);
+      }
+    }
     if (xmode == 0)
       return make_float2(rl_ratio(g.at(2 * m, y, z), b.x),
                          rl_ratio(g.at(2 * m + 1, y, z), b.y));
@@ -312,11 +369,28 @@ struct MidRLRatio {
     return {nullptr, 0};
   }
   __device__ __forceinline__ float* out_row(int, int) const { return nullptr; }
-  __device__ __forceinline__ float2 apply_s(int m, int, int, float2 b, float* sr, int n) const {
+  __device__ __forceinline__ float2 apply_s(int m, int, int, float2 b, float* sr, int n) {
     const int x = 2 * m;
-    return make_float2(rl_ratio(x < n ? sr[x] : 0.f, b.x), rl_ratio(x + 1 < n ? sr[x + 1] : 0.f, b.y));
+    const float a0 = x < n ? sr[x] : 0.f, a1 = x + 1 < n ? sr[x + 1] : 0.f;
+    if (idiv_partial) {
+      if (x < n) idiv_add(a0, b.x);
+      if (x + 1 < n) idiv_add(a1, b.y);
+    }
+    return make_float2(rl_ratio(a0, b.x), rl_ratio(a1, b.y));
   }
-  __device__ __forceinline__ void finish() {}
+  __device__ __forceinline__ void finish() {
+    if (idiv_partial) {
+      block_sum_store(acc, idiv_partial);
+      if (nblocks && blockIdx.x == 0 && threadIdx.x == 0) *nblocks = (int)gridDim.x;
+    }
+  }
+  // a block that returned early (plane outside the image) contributes zero
+  __device__ __forceinline__ void finish_skipped() {
+    if (idiv_partial && threadIdx.x == 0) {
+      idiv_partial[blockIdx.x] = 0.0;
+      if (nblocks && blockIdx.x == 0) *nblocks = (int)gridDim.x;
+    }
+  }
 };
 
 // JVC update (src/JansenVanCittertDeconvolve.cxx:106-111,

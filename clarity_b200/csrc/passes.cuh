@@ -530,7 +530,10 @@ __global__ void __launch_bounds__(256, 2)
   const float2* twx = tw + P.ax.tw_off;
   // a plane whose result is known to be zero is neither read nor written;
   // the next Z pass reads those planes as zeros (Mod::zn)
-  if (mid.zero_plane(z)) return;
+  if (mid.zero_plane(z)) {  // neither read nor written (see Mod::zn)
+    if constexpr (requires { mid.finish_skipped(); }) mid.finish_skipped();
+    return;
+  }
   cols_rt<false>(sm, P, S, z, y0base, tw, xrev);
   __syncthreads();
   smem_inverse<true>(sm, P, P.ax, 1, P.G * P.Ay, P.G * P.Ay, P.rowStride, 0, 1, false, twx);

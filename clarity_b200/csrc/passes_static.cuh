@@ -66,7 +66,9 @@ struct Shape {
   // bank conflicts.
   static constexpr bool Y_PER_LINE = BY <= 32;
   static constexpr int ZS = BW + W;
-  static constexpr int Z2_SMEM = NZ * ZS * 8;
+  // padded tile, then the z twiddle table w_nz^t (NZ entries)
+  static constexpr int Z2_TILE_BYTES = NZ * ZS * 8;
+  static constexpr int Z2_SMEM = Z2_TILE_BYTES + NZ * 8;
 };
 
 template <class SH>
@@ -579,7 +581,10 @@ __global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
   const int y0base = (blockIdx.x - z * SH::NGROUPS) * SH::G;
   // a plane whose result is known to be zero is neither read nor written;
   // the next Z pass reads those planes as zeros (Mod::zn)
-  if (mid.zero_plane(z)) return;
+  if (mid.zero_plane(z)) {  // neither read nor written (see Mod::zn)
+    if constexpr (requires { mid.finish_skipped(); }) mid.finish_skipped();
+    return;
+  }
   prefetch_tile_rows<SH>(mid, z, y0base);
   const RowSkip<SH, Mid> skip{mid, z, y0base};
   cols_inverse<SH>(sm, S, z, y0base, T.twr, T.twny);
@@ -684,12 +689,12 @@ __device__ __forceinline__ void z2_pass(float2* sm, const float2* __restrict__ t
       dft<R, -1>(v);
       if (span > 1 && i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k * twstep]));
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], tw[i * k * twstep]);
       }
     } else {
       if (span > 1 && i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k * twstep]));
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], tw[i * k * twstep]);
       }
       dft<R, +1>(v);
     }
@@ -749,6 +754,11 @@ __global__ void __launch_bounds__(256, 2)
   const unsigned gbase = blockIdx.x * (unsigned)SH::TILE;
   const int zn = mod.zn < NZ ? mod.zn : NZ;  // planes z >= zn are zero
   if (threadIdx.x < 16) mod.prefetch_tile(gbase, SH::TILE, threadIdx.x, 16);
+  // z twiddles in shared memory: a z-pass task's twiddle is the same for all
+  // lanes of a warp (a broadcast), where the table in global memory cost an
+  // L1 round trip per twiddle
+  float2* twz = sm + SH::Z2_TILE_BYTES / 8;
+  for (int t = threadIdx.x; t < NZ; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) twz[t] = __ldg(&T.twz[t]);
   __shared__ alignas(8) uint64_t bar;
   if constexpr (BULK) {
     static_assert((BW * 8) % 16 == 0 && (ZS * 8) % 16 == 0 && (SH::TILE * 8) % 16 == 0,
@@ -795,22 +805,22 @@ __global__ void __launch_bounds__(256, 2)
   }
   __syncthreads();
   if constexpr (A::npass >= 2) {
-    z2_pass<SH, 0, -1>(sm, T.twz);
+    z2_pass<SH, 0, -1>(sm, twz);
     __syncthreads();
   }
   if constexpr (A::npass >= 3) {
-    z2_pass<SH, 1, -1>(sm, T.twz);
+    z2_pass<SH, 1, -1>(sm, twz);
     __syncthreads();
   }
   z2_last<SH>(sm, mod, gbase, Sout);
   if constexpr (!Mod::forward_only) {
     __syncthreads();
     if constexpr (A::npass >= 3) {
-      z2_pass<SH, 1, +1>(sm, T.twz);
+      z2_pass<SH, 1, +1>(sm, twz);
       __syncthreads();
     }
     if constexpr (A::npass >= 2) {
-      z2_pass<SH, 0, +1>(sm, T.twz);
+      z2_pass<SH, 0, +1>(sm, twz);
       __syncthreads();
     }
     // y0 inverse per line

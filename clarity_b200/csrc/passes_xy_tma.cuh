@@ -344,7 +344,10 @@ __global__ void __launch_bounds__(256, 3)
   constexpr int NB = SH::BY / X::TG;
   const int z = blockIdx.x / NB;
   const int y0base = (blockIdx.x - z * NB) * X::TG;
-  if (epi.zero_plane(z)) return;  // neither read nor written (see Mod::zn)
+  if (epi.zero_plane(z)) {  // neither read nor written (see Mod::zn)
+    if constexpr (requires { epi.finish_skipped(); }) epi.finish_skipped();
+    return;
+  }
   if (!smem_aligned128(buf)) {    // never expected: refuse rather than fault
     if (threadIdx.x == 0) atomicExch(T.err, kErrMisaligned);
     return;

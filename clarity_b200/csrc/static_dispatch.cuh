@@ -32,10 +32,7 @@ inline st::Tables tables_of(const PlanEntry& pe) {
 
 template <class K>
 inline cudaError_t allow_smem_st(K kernel, int smem) {
-  if (smem > 48 * 1024)
-    return cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  return cudaSuccess;
+  return smem_opt_in(reinterpret_cast<const void*>(kernel), smem);
 }
 
 // The TMA XY pass (passes_xy_tma.cuh) serves epilogues with a staged form
@@ -68,8 +65,16 @@ inline bool try_xy_tma(const PlanEntry& pe, cudaStream_t st, const F& fn, const 
   using X = st::XyTma<SH>;
   if constexpr (X::OK && xy_staged<F>()) {
     if (!xy_tma_enabled()) return false;
-    TensorMap tm;
-    if (!encode_s_map<SH>(&tm, S)) return false;
+    // the map depends only on S: encoded once per buffer
+    static thread_local const float2* map_s = nullptr;
+    static thread_local TensorMap tm;
+    if (S != map_s) {
+      if (!encode_s_map<SH>(&tm, S)) {
+        map_s = nullptr;
+        return false;
+      }
+      map_s = S;
+    }
     auto k = st::ks_xy_tma<SH, F, FUSE>;
     *err = allow_smem_st(k, X::SMEM);
     if (*err != cudaSuccess) return true;

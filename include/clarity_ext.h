@@ -43,6 +43,29 @@ CLARITY_API ClarityResult_t clarityx_wiener_device(
 CLARITY_API ClarityResult_t clarityx_ml_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+/* Richardson-Lucy (Clarity.h.in:337-341) resumed from `start`, an estimate of
+ * imageDim voxels on the device (NULL: the image, as the reference), with an
+ * optional I-divergence trace: when idiv is not NULL, idiv[k] (device doubles,
+ * `iterations` + 1 of them) receives sum g ln(g/b) + b - g over the image, b =
+ * kernel * (the estimate at the start of iteration k), accumulated in FP64 by
+ * the ratio pass at no extra pass over memory; idiv[iterations] is the
+ * result's own (one more convolution). */
+CLARITY_API ClarityResult_t clarityx_ml_ex_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, const float *start, float *out, int iterations,
+    double *idiv, void *stream);
+
+/* Accelerated Richardson-Lucy: the update and flux rescale of
+ * Clarity_MaximumLikelihoodDeconvolve applied at extrapolated points
+ * y = max(0, x + alpha (x - x_prev)), alpha from the last two steps (vector
+ * extrapolation of Biggs and Andrews, Applied Optics 36(8):1766-1775, 1997).
+ * No reference counterpart.  idiv as clarityx_ml_ex_device (entries before the
+ * last taken at the extrapolated points). */
+CLARITY_API ClarityResult_t clarityx_ml_accel_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, int iterations, double *idiv,
+    void *stream);
+
 /* Richardson-Lucy on `count` independent volumes of any sizes (device
  * pointers, one kernel per volume): each volume has its own plan and
  * workspace and the volumes run concurrently on a pool of streams, forked

@@ -81,6 +81,18 @@ class Oracle:
                 extra64 = [i]  # no sum mode: always double
             fn64.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p] + extra64 + [C.c_void_p]
             fn64.restype = None
+        L.oracle_rl_ex_f32.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, i, i,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_rl_ex_f32.restype = None
+        L.oracle_rl_ex_f64.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, i,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_rl_ex_f64.restype = None
+        L.oracle_rl_accel_f32.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, i, i,
+                                          C.c_void_p]
+        L.oracle_rl_accel_f32.restype = None
+        L.oracle_rl_accel_f64.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, i,
+                                          C.c_void_p]
+        L.oracle_rl_accel_f64.restype = None
         L.oracle_idivergence.argtypes = [_f32p, _f32p, C.c_long, C.POINTER(C.c_long)]
         L.oracle_idivergence.restype = C.c_double
         L.oracle_pad_shift.argtypes = [_f32p, i, i, i, _f32p, i, i, i,
@@ -112,6 +124,40 @@ class Oracle:
     def rl(self, img, psf, iters, precision="f32", sum_mode=SUM_DOUBLE, work=False):
         extra = [iters, sum_mode] if precision == "f32" else [iters]
         return self._run("rl", img, psf, extra, precision, work)
+
+    def rl_ex(self, img, psf, iters, start=None, precision="f32", sum_mode=SUM_DOUBLE):
+        """RL from `start` (image-shaped; None: the image); returns (out, idiv
+        trace of `iters` + 1 entries: per iteration start, then the result)."""
+        img, psf = _f32(img), _f32(psf)
+        out = np.empty_like(img)
+        st = _f32(start) if start is not None else None
+        tr = np.zeros(max(int(iters), 0) + 1, np.float64)
+        ix, iy, iz = _dims(img)
+        kx, ky, kz = _dims(psf)
+        sp = st.ctypes.data if st is not None else None
+        if precision == "f32":
+            self.lib.oracle_rl_ex_f32(img, ix, iy, iz, psf, kx, ky, kz, out, int(iters),
+                                      int(sum_mode), sp, tr.ctypes.data, None)
+        else:
+            self.lib.oracle_rl_ex_f64(img, ix, iy, iz, psf, kx, ky, kz, out, int(iters),
+                                      sp, tr.ctypes.data, None)
+        return out, tr
+
+    def rl_accel(self, img, psf, iters, precision="f32", sum_mode=SUM_DOUBLE):
+        """Accelerated RL (Biggs-Andrews); returns (out, idiv trace of
+        `iters` + 1 entries: at each extrapolated point, then the result)."""
+        img, psf = _f32(img), _f32(psf)
+        out = np.empty_like(img)
+        tr = np.zeros(max(int(iters), 0) + 1, np.float64)
+        ix, iy, iz = _dims(img)
+        kx, ky, kz = _dims(psf)
+        if precision == "f32":
+            self.lib.oracle_rl_accel_f32(img, ix, iy, iz, psf, kx, ky, kz, out, int(iters),
+                                         int(sum_mode), tr.ctypes.data)
+        else:
+            self.lib.oracle_rl_accel_f64(img, ix, iy, iz, psf, kx, ky, kz, out, int(iters),
+                                         tr.ctypes.data)
+        return out, tr
 
     def wiener(self, img, psf, eps, precision="f32", work=False):
         return self._run("wiener", img, psf, [eps], precision, work)

@@ -96,6 +96,8 @@ def test_emulated_library_matches_oracle(emu, tmp_path, oracle_lib, img_zyx, psf
                   oracle_lib.wiener(img, psf, 1e-2)) <= 2e-6
     assert rel_l2(run_emu(emu, tmp_path, "sjvc", img, psf, 3),
                   oracle_lib.smoothed_jvc(img, psf, 3, 2, (1.0, 1.5, 0.7))) <= 2e-6
+    out, _ = oracle_lib.rl_accel(img, psf, 4)
+    assert rel_l2(run_emu(emu, tmp_path, "accel", img, psf, 4), out) <= 2e-6
     # batched RL: three volumes, each identical to its own solve (checked in
     # emu_main), the first against the oracle
     assert rel_l2(run_emu(emu, tmp_path, "batch", img, psf, 2),

@@ -233,3 +233,68 @@ def test_autotuned_plan_matches_oracle(clarity_gpu, oracle_lib):
     finally:
         clarity_gpu.autotune(False)
     assert rel_l2(out, oracle_lib.rl(img[0], psf[0], 3)) <= TOL_ITER
+
+
+@pytest.mark.parametrize("case", ["small_even", "cfg0_rl10"])
+def test_idiv_trace_and_resume_vs_oracle(clarity_gpu, oracle_lib, case):
+    # the I-divergence trace accumulated by the ratio pass, and RL resumed from
+    # a given estimate, against the oracle's restatement of both
+    import torch
+    d = load_golden(case)
+    img, psf = d["image"], d["psf"]
+    iters = 4
+    di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
+    out = torch.empty_like(di)
+    tr = torch.zeros(iters + 1, dtype=torch.float64, device="cuda")
+    clarity_gpu.ml_ex_device(di, dk, out, iters, idiv=tr)
+    torch.cuda.synchronize()
+    ref_out, ref_tr = oracle_lib.rl_ex(img, psf, iters)
+    assert rel_l2(out.cpu().numpy(), ref_out) <= TOL_ITER
+    np.testing.assert_allclose(tr.cpu().numpy(), ref_tr, rtol=1e-4)
+    # start = the image is plain RL, bit for bit
+    plain = torch.empty_like(di)
+    clarity_gpu.ml_device(di, dk, plain, iters)
+    torch.cuda.synchronize()
+    assert torch.equal(plain, out)
+    # resume from a smoothed estimate
+    start = np.ascontiguousarray(0.5 * img + 0.5 * float(img.mean()), np.float32)
+    res = torch.empty_like(di)
+    tr2 = torch.zeros(iters + 1, dtype=torch.float64, device="cuda")
+    clarity_gpu.ml_ex_device(di, dk, res, iters, start=torch.from_numpy(start).cuda(), idiv=tr2)
+    torch.cuda.synchronize()
+    ref_res, ref_tr2 = oracle_lib.rl_ex(img, psf, iters, start=start)
+    assert rel_l2(res.cpu().numpy(), ref_res) <= TOL_ITER
+    np.testing.assert_allclose(tr2.cpu().numpy(), ref_tr2, rtol=1e-4)
+
+
+def test_cfg1_idiv_trace_vs_oracle(clarity_gpu, oracle_lib):
+    # full size: the trace through the TMA ratio pass
+    import torch
+    img, psf, _ = syn.cfg1(seed=4)
+    di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
+    out = torch.empty_like(di)
+    tr = torch.zeros(3, dtype=torch.float64, device="cuda")
+    clarity_gpu.ml_ex_device(di, dk, out, 2, idiv=tr)
+    torch.cuda.synchronize()
+    _, ref_tr = oracle_lib.rl_ex(img, psf, 2)
+    np.testing.assert_allclose(tr.cpu().numpy(), ref_tr, rtol=1e-4)
+
+
+@pytest.mark.parametrize("case", ["small_even", "cfg0_rl10"])
+def test_accelerated_rl_vs_oracle(clarity_gpu, oracle_lib, case):
+    # Biggs-Andrews extrapolated RL against the oracle's restatement, with the
+    # I-divergence trace (at the extrapolated points, then the result)
+    import torch
+    d = load_golden(case)
+    img, psf = d["image"], d["psf"]
+    iters = 8
+    di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
+    out = torch.empty_like(di)
+    tr = torch.zeros(iters + 1, dtype=torch.float64, device="cuda")
+    clarity_gpu.ml_accel_device(di, dk, out, iters, idiv=tr)
+    torch.cuda.synchronize()
+    ref, ref_tr = oracle_lib.rl_accel(img, psf, iters)
+    assert rel_l2(out.cpu().numpy(), ref) <= TOL_ITER
+    np.testing.assert_allclose(tr.cpu().numpy(), ref_tr, rtol=1e-4)
+    ref64, _ = oracle_lib.rl_accel(img, psf, iters, precision="f64")
+    assert rel_l2(out.cpu().numpy(), ref64) <= 1e-3
