@@ -195,6 +195,56 @@ NCU_TRAFFIC = {"xy_product": 278.6e6 + 223.9e6, "xy_inv_fwd": 85.1e6 + 33.1e6,
                "z": (271.5e6 + 87.8e6 + 203.5e6 + 87.8e6) / 2}
 
 
+def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=60):
+    """The second metric: device time until I-div(g, h*u) is within 1% of
+    plain RL's value after `plain_iters` iterations, for plain RL and for the
+    chosen form (Biggs-Andrews accelerated RL), on the same GPU and inputs.
+    The I-divergence of every plain iterate comes from the trace the ratio
+    pass accumulates; the chosen form's iteration count is the smallest whose
+    result meets the target (its own traced final I-divergence)."""
+    out = torch.empty_like(img_d)
+    tr = torch.zeros(plain_iters + 1, dtype=torch.float64, device="cuda")
+    api.ml_ex_device(img_d, psf_d, out, plain_iters, idiv=tr, stream=stream)
+    torch.cuda.synchronize()
+    t = tr.cpu().numpy()
+    target = 1.01 * float(t[plain_iters])
+    k_plain = int(np.argmax(t <= target))
+    k_acc, finals = None, {}
+    for k in range(2, max_accel + 1):
+        ta = torch.zeros(k + 1, dtype=torch.float64, device="cuda")
+        api.ml_accel_device(img_d, psf_d, out, k, idiv=ta, stream=stream)
+        torch.cuda.synchronize()
+        finals[k] = float(ta[k].item())
+        if finals[k] <= target:
+            k_acc = k
+            break
+
+    def ev_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    res = {"target": "I-divergence within 1% of plain RL after 200 iterations",
+           "idiv_plain_200": float(t[plain_iters]), "idiv_target": target,
+           "plain": {"iterations": k_plain,
+                     "ms": ev_ms(lambda: api.ml_device(img_d, psf_d, out, k_plain, stream))},
+           "chosen": {"form": "accelerated RL (Biggs-Andrews vector extrapolation)",
+                      "iterations": k_acc}}
+    if k_acc:
+        res["chosen"]["ms"] = ev_ms(lambda: api.ml_accel_device(img_d, psf_d, out, k_acc,
+                                                                stream=stream))
+        res["chosen"]["idiv"] = finals[k_acc]
+        res["speedup"] = res["plain"]["ms"] / res["chosen"]["ms"]
+    return res
+
+
 def run_gpu_arm(args, rank, world):
     import torch
     from clarity_b200 import api, synthetic as syn
@@ -315,6 +365,8 @@ def run_gpu_arm(args, rank, world):
                     "GBps": (fb[k] / v[1]) / (v[0] / v[1] / 1e3) / 1e9}
                 for k, v in fam_ms.items()}
 
+    ttt = time_to_target(api, torch, img_d, psf_d, stream) if rank == 0 else None
+
     if rank == 0:
         sample_iters = max(1, args.cpu_iters)
         t_cpu, kind, cores = cpu_reference_rl(img, psf, sample_iters)
@@ -345,6 +397,7 @@ def run_gpu_arm(args, rank, world):
                              "sample": f"RL on the same 256x256x64 workload, {sample_iters} "
                                        f"iteration(s), {cores} host threads"},
             "clocks": clk,
+            "time_to_target": ttt,
         }
         print(json.dumps(line), flush=True)
     api.unregister()
