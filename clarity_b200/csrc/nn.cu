@@ -1,0 +1,778 @@
+// nn.cu -- kernels of the learned-start network: a 3-D U-Net on channels-last
+// BF16 activations with FP32 accumulation.
+//
+// * conv3: 3x3x3 convolution (zero padding 1) as an implicit GEMM on the
+//   tensor cores (mma.sync m16n8k16 bf16 -> f32).  M = voxels (128 per block),
+//   N = output channels, K = 27 taps x input channels.  The input may be the
+//   concatenation of a full-resolution tensor and a half-resolution tensor read
+//   through nearest upsampling (the decoder's skip + up path), so neither the
+//   upsampled nor the concatenated tensor is ever stored.  A- and B-tiles move
+//   global -> shared by cp.async (zero-fill at the volume border) in a two-stage
+//   pipeline, fragments by ldmatrix.  Epilogue: bias, ReLU, or a ReLU-derivative
+//   mask (backward data), BF16 store.  The backward data pass is the same
+//   kernel with the mirrored, transposed weights.
+// * conv3_wgrad: dW[co][tap][ci] = sum_v dy[v][co] in(v + tap)[ci], the same
+//   implicit-GEMM tiles with K = voxels, split over blocks and summed with FP32
+//   atomics.
+// * SIMT kernels: the 1 -> 16 input convolution, the 16 -> 1 head with the loss,
+//   pooling, the gradient merges, bias sums, Adam, weight packing.
+//
+// Layout: activation [v][c], v = (z*H + y)*W + x; weights [co][tap][ci] with
+// tap = (dz+1)*9 + (dy+1)*3 + (dx+1).  Channel counts of the tensor-core
+// kernels are multiples of 16.
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "engine.hpp"
+#include "launch_macro.cuh"
+
+namespace clarity {
+namespace nn {
+
+using bf16 = __nv_bfloat16;
+
+struct Conv3Args {
+  const bf16* x1;  // full-resolution input [v][c1]
+  int c1;
+  const bf16* x2;  // optional half-resolution input [u][c2] (nearest upsampled), or nullptr
+  int c2;
+  int D, H, W;     // output (= full-resolution input) dims
+  int D2, H2, W2;  // x2 dims
+  const bf16* w;   // [cout][27][c1 + c2]
+  const float* bias;
+  int cout;
+  int relu;
+  const bf16* mask;  // optional [v][cout]: result *= (mask > 0)
+  bf16* y;           // [v][cout]
+};
+
+constexpr int kBM = 128;   // voxels per block
+constexpr int kRow = 24;   // smem row pitch in bf16 (48 B: conflict-free ldmatrix)
+
+__device__ __forceinline__ void tap_offset(int t, int* dz, int* dy, int* dx) {
+  *dz = t / 9 - 1;
+  *dy = (t / 3) % 3 - 1;
+  *dx = t % 3 - 1;
+}
+
+// Source of 8 consecutive input channels [c, c+8) at shifted voxel
+// (z, y, x); nullptr outside the volume (zero padding).
+__device__ __forceinline__ const bf16* in_chunk(const Conv3Args& a, int z, int y, int x, int c) {
+  if (z < 0 || y < 0 || x < 0 || z >= a.D || y >= a.H || x >= a.W) return nullptr;
+  if (c < a.c1) return a.x1 + ((size_t)((z * a.H + y) * a.W + x) * a.c1 + c);
+  const int zz = z >> 1, yy = y >> 1, xx = x >> 1;
+  return a.x2 + ((size_t)((zz * a.H2 + yy) * a.W2 + xx) * a.c2 + (c - a.c1));
+}
+
+#ifndef CLARITY_HOST_EMULATION
+__device__ __forceinline__ uint32_t su32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+// 16-byte global -> shared copy; src nullptr -> zero fill
+__device__ __forceinline__ void cp16(void* dst, const void* src, const void* any_valid) {
+  const int n = src ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(su32(dst)),
+               "l"(src ? src : any_valid), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void ldm_x4(uint32_t* r, const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(su32(p)));
+}
+__device__ __forceinline__ void ldm_x4_t(uint32_t* r, const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(su32(p)));
+}
+__device__ __forceinline__ void mma16816(float* c, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+#else
+inline void cp16(void* dst, const void* src, const void*) {
+  if (src) std::memcpy(dst, src, 16);
+  else std::memset(dst, 0, 16);
+}
+inline void cp_commit() {}
+template <int N>
+inline void cp_wait() {}
+#endif
+
+// out[v][co] = sum_{tap, c} in(v + tap)[c] w[co][tap][c] (+ bias, ReLU / mask).
+// Grid (ceil(V / 128), cout / BN), 128 threads; warp w owns voxel rows
+// [32w, 32w + 32) and all BN channels of the block.
+template <int BN>
+__global__ void __launch_bounds__(128) k_conv3(const Conv3Args a) {
+  static_assert(BN % 16 == 0 && BN <= 64, "BN: 16, 32, 48 or 64");
+  __shared__ alignas(128) bf16 As[2][kBM * kRow];
+  __shared__ alignas(128) bf16 Bs[2][BN * kRow];
+  const int cin = a.c1 + a.c2;
+  const int nsteps = 27 * (cin / 16);
+  const long long V = (long long)a.D * a.H * a.W;
+  const long long v0 = (long long)blockIdx.x * kBM;
+  const int co0 = blockIdx.y * BN;
+
+  auto load = [&](int s, int stage) {
+    const int t = s / (cin / 16), cc = s - t * (cin / 16);
+    int dz, dy, dx;
+    tap_offset(t, &dz, &dy, &dx);
+    for (int q = threadIdx.x; q < 2 * kBM; q += CLARITY_BLOCK_STRIDE(128)) {
+      const int r = q >> 1, half = q & 1;
+      const long long v = v0 + r;
+      const bf16* src = nullptr;
+      if (v < V) {
+        const int x = (int)(v % a.W);
+        const long long zy = v / a.W;
+        const int y = (int)(zy % a.H), z = (int)(zy / a.H);
+        src = in_chunk(a, z + dz, y + dy, x + dx, cc * 16 + half * 8);
+      }
+      cp16(&As[stage][r * kRow + half * 8], src, a.x1);
+    }
+    for (int q = threadIdx.x; q < 2 * BN; q += CLARITY_BLOCK_STRIDE(128)) {
+      const int n = q >> 1, half = q & 1;
+      const bf16* src = a.w + ((size_t)(co0 + n) * 27 + t) * cin + cc * 16 + half * 8;
+      cp16(&Bs[stage][n * kRow + half * 8], src, a.x1);
+    }
+    cp_commit();
+  };
+
+#ifndef CLARITY_HOST_EMULATION
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float acc[2][BN / 8][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < BN / 8; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+  load(0, 0);
+  for (int s = 0; s < nsteps; ++s) {
+    const int st = s & 1;
+    if (s + 1 < nsteps) {
+      load(s + 1, st ^ 1);
+      cp_wait<1>();
+    } else {
+      cp_wait<0>();
+    }
+    __syncthreads();
+    uint32_t af[2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      ldm_x4(af[i], &As[st][(warp * 32 + i * 16 + (lane & 15)) * kRow + (lane >> 4) * 8]);
+#pragma unroll
+    for (int j = 0; j < BN / 8; j += 2) {
+      uint32_t bfr[4];
+      ldm_x4(bfr, &Bs[st][(j * 8 + (lane & 7) + (lane >> 4) * 8) * kRow + ((lane >> 3) & 1) * 8]);
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        mma16816(acc[i][j], af[i], bfr);
+        mma16816(acc[i][j + 1], af[i], bfr + 2);
+      }
+    }
+    __syncthreads();
+  }
+  // epilogue: acc[i][j] holds rows g, g+8 (g = lane/4) and columns 2(lane%4), +1
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < BN / 8; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long long v = v0 + warp * 32 + i * 16 + (lane >> 2) + h * 8;
+        const int co = co0 + j * 8 + (lane & 3) * 2;
+        if (v >= V) continue;
+        float r0 = acc[i][j][2 * h], r1 = acc[i][j][2 * h + 1];
+        if (a.bias) {
+          r0 += a.bias[co];
+          r1 += a.bias[co + 1];
+        }
+        if (a.relu) {
+          r0 = fmaxf(r0, 0.f);
+          r1 = fmaxf(r1, 0.f);
+        }
+        const size_t o = (size_t)v * a.cout + co;
+        if (a.mask) {
+          const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162*>(a.mask + o);
+          if (!(__bfloat162float(m.x) > 0.f)) r0 = 0.f;
+          if (!(__bfloat162float(m.y) > 0.f)) r1 = 0.f;
+        }
+        *reinterpret_cast<__nv_bfloat162*>(a.y + o) = __floats2bfloat162_rn(r0, r1);
+      }
+#else
+  // host emulation: the same tiles, multiplied with scalar loops
+  static thread_local float accs[kBM][64];
+  for (int r = 0; r < kBM; ++r)
+    for (int n = 0; n < BN; ++n) accs[r][n] = 0.f;
+  for (int s = 0; s < nsteps; ++s) {
+    load(s, 0);
+    for (int r = 0; r < kBM; ++r)
+      for (int n = 0; n < BN; ++n) {
+        float t = 0.f;
+        for (int k = 0; k < 16; ++k)
+          t += __bfloat162float(As[0][r * kRow + k]) * __bfloat162float(Bs[0][n * kRow + k]);
+        accs[r][n] += t;
+      }
+  }
+  for (int r = 0; r < kBM; ++r) {
+    const long long v = v0 + r;
+    if (v >= V) continue;
+    for (int n = 0; n < BN; ++n) {
+      const int co = co0 + n;
+      float x = accs[r][n];
+      if (a.bias) x += a.bias[co];
+      if (a.relu) x = fmaxf(x, 0.f);
+      const size_t o = (size_t)v * a.cout + co;
+      if (a.mask && !(__bfloat162float(a.mask[o]) > 0.f)) x = 0.f;
+      a.y[o] = __float2bfloat16_rn(x);
+    }
+  }
+#endif
+}
+
+// dW[co][tap][ci] += sum over this block's voxels of dy[v][co] in(v + tap)[ci]
+// (FP32 atomics; the caller zeroes dW).  GEMM M = cout (BM rows per block),
+// N = 27 cin (64 columns per block: four 16-channel groups, each one tap),
+// K = voxels (16 per step, kVoxChunk per block).  Warp w owns columns
+// [16w, 16w + 16) of the block for all BM rows.
+constexpr int kVoxChunk = 2048;
+constexpr int kWRow = 72;  // smem pitch (bf16) of the [voxel][64] tiles: conflict-free
+
+template <int BM>
+__global__ void __launch_bounds__(128) k_conv3_wgrad(const Conv3Args a, const bf16* __restrict__ dy,
+                                                    float* __restrict__ dw) {
+  static_assert(BM % 16 == 0 && BM <= 64, "BM: 16, 32, 48 or 64");
+  __shared__ alignas(128) bf16 As[2][16 * kWRow];  // [voxel][co]
+  __shared__ alignas(128) bf16 Bs[2][16 * kWRow];  // [voxel][n]
+  const int cin = a.c1 + a.c2;
+  const int ngroups = 27 * (cin / 16);
+  const int N = 27 * cin;
+  const long long V = (long long)a.D * a.H * a.W;
+  const int nb = blockIdx.x;           // 64-column block
+  const int co0 = blockIdx.y * BM;
+  const long long vbeg = (long long)blockIdx.z * kVoxChunk;
+  const long long vend = vbeg + kVoxChunk < V ? vbeg + kVoxChunk : V;
+  const int nsteps = (int)((vend - vbeg + 15) / 16);
+
+  auto load = [&](int s, int stage) {
+    const long long vb = vbeg + (long long)s * 16;
+    // A: 16 voxels x BM channels of dy, BM/8 chunks per voxel
+    for (int q = threadIdx.x; q < 16 * (BM / 8); q += CLARITY_BLOCK_STRIDE(128)) {
+      const int r = q / (BM / 8), ch = q - r * (BM / 8);
+      const long long v = vb + r;
+      const bf16* src = v < vend ? dy + ((size_t)v * a.cout + co0 + ch * 8) : nullptr;
+      cp16(&As[stage][r * kWRow + ch * 8], src, dy);
+    }
+    // B: 16 voxels x 4 groups x 2 halves of the shifted input
+    for (int q = threadIdx.x; q < 16 * 8; q += CLARITY_BLOCK_STRIDE(128)) {
+      const int r = q >> 3, gi = (q >> 1) & 3, half = q & 1;
+      const int gg = nb * 4 + gi;
+      const long long v = vb + r;
+      const bf16* src = nullptr;
+      if (v < vend && gg < ngroups) {
+        const int t = gg / (cin / 16), cc = gg - t * (cin / 16);
+        int dz, dyo, dx;
+        tap_offset(t, &dz, &dyo, &dx);
+        const int x = (int)(v % a.W);
+        const long long zy = v / a.W;
+        const int y = (int)(zy % a.H), z = (int)(zy / a.H);
+        src = in_chunk(a, z + dz, y + dyo, x + dx, cc * 16 + half * 8);
+      }
+      cp16(&Bs[stage][r * kWRow + gi * 16 + half * 8], src, a.x1);
+    }
+    cp_commit();
+  };
+
+#ifndef CLARITY_HOST_EMULATION
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float acc[BM / 16][2][4];
+#pragma unroll
+  for (int i = 0; i < BM / 16; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+  if (nsteps > 0) load(0, 0);
+  for (int s = 0; s < nsteps; ++s) {
+    const int st = s & 1;
+    if (s + 1 < nsteps) {
+      load(s + 1, st ^ 1);
+      cp_wait<1>();
+    } else {
+      cp_wait<0>();
+    }
+    __syncthreads();
+    // B fragments of the warp's two n8 tiles: stored [k][n], transposed load
+    uint32_t bfr[4];
+    ldm_x4_t(bfr, &Bs[st][((lane & 7) + ((lane >> 3) & 1) * 8) * kWRow + warp * 16 + (lane >> 4) * 8]);
+#pragma unroll
+    for (int i = 0; i < BM / 16; ++i) {
+      // A fragment (rows co, cols voxel) from the stored [voxel][co] tile
+      uint32_t af[4];
+      ldm_x4_t(af, &As[st][((lane & 7) + (lane >> 4) * 8) * kWRow + i * 16 + ((lane >> 3) & 1) * 8]);
+      mma16816(acc[i][0], af, bfr);
+      mma16816(acc[i][1], af, bfr + 2);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < BM / 16; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int co = co0 + i * 16 + (lane >> 2) + h * 8;
+        const int nl = warp * 16 + j * 8 + (lane & 3) * 2;  // column in the block
+        const int gg = nb * 4 + (nl >> 4);
+        if (gg >= ngroups) continue;
+        const int n = nb * 64 + nl;
+        atomicAdd(&dw[(size_t)co * N + n], acc[i][j][2 * h]);
+        atomicAdd(&dw[(size_t)co * N + n + 1], acc[i][j][2 * h + 1]);
+      }
+#else
+  static thread_local float accs[64][64];
+  for (int m = 0; m < BM; ++m)
+    for (int n = 0; n < 64; ++n) accs[m][n] = 0.f;
+  for (int s = 0; s < nsteps; ++s) {
+    load(s, 0);
+    for (int m = 0; m < BM; ++m)
+      for (int n = 0; n < 64; ++n) {
+        float t = 0.f;
+        for (int k = 0; k < 16; ++k)
+          t += __bfloat162float(As[0][k * kWRow + m]) * __bfloat162float(Bs[0][k * kWRow + n]);
+        accs[m][n] += t;
+      }
+  }
+  for (int m = 0; m < BM; ++m)
+    for (int n = 0; n < 64; ++n) {
+      const int gg = nb * 4 + (n >> 4);
+      if (gg >= ngroups) continue;
+      dw[(size_t)(co0 + m) * N + nb * 64 + n] += accs[m][n];
+    }
+#endif
+}
+
+// ------------------------------------------------------------- SIMT kernels
+// Input layer: y[v][co] = relu(b[co] + sum_tap w[co][tap] x(v + tap)), 16 outputs.
+__global__ void k_conv_in(const float* __restrict__ x, int D, int H, int W,
+                          const float* __restrict__ w, const float* __restrict__ b,
+                          bf16* __restrict__ y) {
+  __shared__ float ws[16 * 27 + 16];
+  for (int i = threadIdx.x; i < 16 * 27; i += blockDim.x) ws[i] = w[i];
+  for (int i = threadIdx.x; i < 16; i += blockDim.x) ws[16 * 27 + i] = b[i];
+  __syncthreads();
+  const long long V = (long long)D * H * W;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int xx = (int)(v % W);
+    const long long zy = v / W;
+    const int yy = (int)(zy % H), zz = (int)(zy / H);
+    float in[27];
+    for (int t = 0; t < 27; ++t) {
+      int dz, dy, dx;
+      tap_offset(t, &dz, &dy, &dx);
+      const int z2 = zz + dz, y2 = yy + dy, x2 = xx + dx;
+      in[t] = (z2 < 0 || y2 < 0 || x2 < 0 || z2 >= D || y2 >= H || x2 >= W)
+                  ? 0.f
+                  : x[((long long)z2 * H + y2) * W + x2];
+    }
+    for (int co = 0; co < 16; co += 2) {
+      float r0 = ws[16 * 27 + co], r1 = ws[16 * 27 + co + 1];
+      for (int t = 0; t < 27; ++t) {
+        r0 += ws[co * 27 + t] * in[t];
+        r1 += ws[(co + 1) * 27 + t] * in[t];
+      }
+      *reinterpret_cast<__nv_bfloat162*>(y + v * 16 + co) =
+          __floats2bfloat162_rn(fmaxf(r0, 0.f), fmaxf(r1, 0.f));
+    }
+  }
+}
+
+// Input-layer gradients: dw[co][tap] += sum_v dy[v][co] x(v + tap), db[co] +=
+// sum_v dy[v][co] (dy already masked by the ReLU derivative).
+__global__ void k_conv_in_wgrad(const float* __restrict__ x, int D, int H, int W,
+                                const bf16* __restrict__ dy, float* __restrict__ dw,
+                                float* __restrict__ db) {
+  __shared__ float red[16 * 28];
+  for (int i = threadIdx.x; i < 16 * 28; i += blockDim.x) red[i] = 0.f;
+  __syncthreads();
+  float acc[16 * 28 / 16];  // each thread accumulates one output channel's 28 sums
+  const int co = threadIdx.x & 15;
+  for (int i = 0; i < 28; ++i) acc[i] = 0.f;
+  const long long V = (long long)D * H * W;
+  for (long long v = blockIdx.x * (long long)(blockDim.x / 16) + (threadIdx.x >> 4); v < V;
+       v += (long long)gridDim.x * (blockDim.x / 16)) {
+    const float g = __bfloat162float(dy[v * 16 + co]);
+    if (g == 0.f) continue;
+    const int xx = (int)(v % W);
+    const long long zy = v / W;
+    const int yy = (int)(zy % H), zz = (int)(zy / H);
+    for (int t = 0; t < 27; ++t) {
+      int dz, dyo, dx;
+      tap_offset(t, &dz, &dyo, &dx);
+      const int z2 = zz + dz, y2 = yy + dyo, x2 = xx + dx;
+      if (z2 < 0 || y2 < 0 || x2 < 0 || z2 >= D || y2 >= H || x2 >= W) continue;
+      acc[t] += g * x[((long long)z2 * H + y2) * W + x2];
+    }
+    acc[27] += g;
+  }
+  for (int i = 0; i < 28; ++i) atomicAdd(&red[co * 28 + i], acc[i]);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 16 * 28; i += blockDim.x) {
+    const int c = i / 28, k = i - c * 28;
+    if (k < 27) atomicAdd(&dw[c * 27 + k], red[i]);
+    else atomicAdd(&db[c], red[i]);
+  }
+}
+
+// Head: r[v] = b + sum_c w[c] y[v][c] (16 channels).
+__global__ void k_head(const bf16* __restrict__ y, long long V, const float* __restrict__ w,
+                       const float* __restrict__ b, float* __restrict__ r) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    float s = b[0];
+    for (int c = 0; c < 16; ++c) s += w[c] * __bfloat162float(y[v * 16 + c]);
+    r[v] = s;
+  }
+}
+
+// Loss L = sum_v (r - t)^2 / V and its gradients: dy[v][c] = dL/dr w[c] masked
+// by y > 0 (the last ReLU), dw[c] += sum dL/dr y[v][c], db += sum dL/dr;
+// loss partial sums (FP64) into *loss by atomics.
+__global__ void k_head_loss_grad(const bf16* __restrict__ y, long long V,
+                                 const float* __restrict__ w, const float* __restrict__ r,
+                                 const float* __restrict__ t, bf16* __restrict__ dy,
+                                 float* __restrict__ dw, float* __restrict__ db,
+                                 double* __restrict__ loss) {
+  float gw[16];
+  for (int c = 0; c < 16; ++c) gw[c] = 0.f;
+  float gb = 0.f;
+  double l = 0;
+  const float inv = 1.f / (float)V;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const float e = r[v] - t[v];
+    l += (double)e * e;
+    const float g = 2.f * e * inv;
+    gb += g;
+    for (int c = 0; c < 16; c += 2) {
+      const float y0 = __bfloat162float(y[v * 16 + c]), y1 = __bfloat162float(y[v * 16 + c + 1]);
+      gw[c] += g * y0;
+      gw[c + 1] += g * y1;
+      *reinterpret_cast<__nv_bfloat162*>(dy + v * 16 + c) =
+          __floats2bfloat162_rn(y0 > 0.f ? g * w[c] : 0.f, y1 > 0.f ? g * w[c + 1] : 0.f);
+    }
+  }
+  for (int c = 0; c < 16; ++c) atomicAdd(&dw[c], gw[c]);
+  atomicAdd(db, gb);
+  atomicAdd(loss, l / (double)V);
+}
+
+// Average pool 2x2x2: y[u][c] = mean of the 8 children (dims even).
+__global__ void k_pool2(const bf16* __restrict__ x, int C, int D, int H, int W,
+                        bf16* __restrict__ y) {
+  const int D2 = D / 2, H2 = H / 2, W2 = W / 2;
+  const long long n = (long long)D2 * H2 * W2 * C;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const long long u = i / C;
+    const int x2 = (int)(u % W2);
+    const long long zy = u / W2;
+    const int y2 = (int)(zy % H2), z2 = (int)(zy / H2);
+    float s = 0.f;
+    for (int k = 0; k < 8; ++k) {
+      const int z = 2 * z2 + (k >> 2), y = 2 * y2 + ((k >> 1) & 1), xx = 2 * x2 + (k & 1);
+      s += __bfloat162float(x[((long long)(z * H + y) * W + xx) * C + c]);
+    }
+    y[i] = __float2bfloat16_rn(0.125f * s);
+  }
+}
+
+// Gradient of a skip tensor s (ReLU output, c channels): (dxcat[v][0..c) if
+// given + dp[parent(v)][c] / 8) * (s > 0).  dxcat has ccat channels.
+__global__ void k_merge_skip_grad(const bf16* __restrict__ dxcat, int ccat,
+                                  const bf16* __restrict__ dp, const bf16* __restrict__ s,
+                                  int c, int D, int H, int W, bf16* __restrict__ out) {
+  const long long n = (long long)D * H * W * c;
+  const int D2 = D / 2, H2 = H / 2, W2 = W / 2;
+  (void)D2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int ch = (int)(i % c);
+    const long long v = i / c;
+    float g = dxcat ? __bfloat162float(dxcat[v * ccat + ch]) : 0.f;
+    if (dp) {
+      const int xx = (int)(v % W);
+      const long long zy = v / W;
+      const int yy = (int)(zy % H), zz = (int)(zy / H);
+      const long long u = ((long long)(zz >> 1) * H2 + (yy >> 1)) * W2 + (xx >> 1);
+      g += 0.125f * __bfloat162float(dp[u * c + ch]);
+    }
+    out[i] = __float2bfloat16_rn(__bfloat162float(s[i]) > 0.f ? g : 0.f);
+  }
+}
+
+// Gradient of the coarse (half-resolution, ReLU output) tensor read through
+// nearest upsampling: sum over the 8 children of dxcat[child][c1 + c], masked
+// by coarse > 0.  (D, H, W): full-resolution dims.
+__global__ void k_up_grad(const bf16* __restrict__ dxcat, int ccat, int c1, int c2,
+                          const bf16* __restrict__ coarse, int D, int H, int W,
+                          bf16* __restrict__ out) {
+  const int D2 = D / 2, H2 = H / 2, W2 = W / 2;
+  const long long n = (long long)D2 * H2 * W2 * c2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % c2);
+    const long long u = i / c2;
+    const int x2 = (int)(u % W2);
+    const long long zy = u / W2;
+    const int y2 = (int)(zy % H2), z2 = (int)(zy / H2);
+    float s = 0.f;
+    for (int k = 0; k < 8; ++k) {
+      const int z = 2 * z2 + (k >> 2), y = 2 * y2 + ((k >> 1) & 1), xx = 2 * x2 + (k & 1);
+      s += __bfloat162float(dxcat[((long long)(z * H + y) * W + xx) * ccat + c1 + c]);
+    }
+    out[i] = __float2bfloat16_rn(__bfloat162float(coarse[i]) > 0.f ? s : 0.f);
+  }
+}
+
+// db[co] += sum_v dy[v][co]
+__global__ void k_bias_grad(const bf16* __restrict__ dy, long long V, int cout,
+                            float* __restrict__ db) {
+  CLARITY_DYN_SMEM(float, sb);
+  for (int i = threadIdx.x; i < cout; i += blockDim.x) sb[i] = 0.f;
+  __syncthreads();
+  const long long n = V * cout;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    atomicAdd(&sb[i % cout], __bfloat162float(dy[i]));
+  __syncthreads();
+  for (int i = threadIdx.x; i < cout; i += blockDim.x) atomicAdd(&db[i], sb[i]);
+}
+
+// Adam (Kingma and Ba, 2015) on FP32 parameters, bias-corrected.
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, long long n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// BF16 weights of one layer from its FP32 master copy [co][27][ci]: the
+// forward layout and the backward-data layout wb[ci][26 - tap][co] (mirrored
+// taps, transposed channels).
+__global__ void k_pack_weights(const float* __restrict__ w, int cout, int cin,
+                               bf16* __restrict__ wf, bf16* __restrict__ wb) {
+  const long long n = (long long)cout * 27 * cin;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int ci = (int)(i % cin);
+    const long long r = i / cin;
+    const int t = (int)(r % 27), co = (int)(r / 27);
+    const bf16 b = __float2bfloat16_rn(w[i]);
+    wf[i] = b;
+    if (wb) wb[((long long)ci * 27 + (26 - t)) * cout + co] = b;
+  }
+}
+
+inline int grid_for(long long n, int threads = 256) {
+  long long g = (n + threads - 1) / threads;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace nn
+}  // namespace clarity
+
+// ==================================================================== C ABI
+using clarity::nn::bf16;
+namespace nnk = clarity::nn;
+
+static int nn_err(cudaError_t e) {
+  if (e == cudaSuccess) return CLARITY_SUCCESS;
+  clarity::set_last_error(cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? CLARITY_DEVICE_OUT_OF_MEMORY : CLARITY_INVALID_OPERATION;
+}
+static int nn_bad(const char* m) {
+  clarity::set_last_error(m);
+  return CLARITY_INVALID_ARGUMENT;
+}
+
+extern "C" {
+
+CLARITY_API ClarityResult_t clarityx_nn_conv3(const void* x1, int c1, const void* x2, int c2,
+                                              int D, int H, int W, const void* w,
+                                              const float* bias, int cout, int relu,
+                                              const void* mask, void* y, void* stream) {
+  if (!x1 || !w || !y || D <= 0 || H <= 0 || W <= 0) return (ClarityResult_t)nn_bad("conv3: argument");
+  if (c1 <= 0 || c1 % 16 || c2 < 0 || c2 % 16 || (c2 && !x2) || cout <= 0 || cout % 16)
+    return (ClarityResult_t)nn_bad("conv3: channel counts must be multiples of 16");
+  if (c2 && (D % 2 || H % 2 || W % 2)) return (ClarityResult_t)nn_bad("conv3: upsampled input needs even dims");
+  if (((uintptr_t)x1 | (uintptr_t)x2 | (uintptr_t)w | (uintptr_t)y | (uintptr_t)mask) & 15)
+    return (ClarityResult_t)nn_bad("conv3: buffers must be 16-byte aligned");
+  nnk::Conv3Args a{static_cast<const bf16*>(x1), c1, static_cast<const bf16*>(x2), c2, D, H, W,
+                   D / 2, H / 2, W / 2, static_cast<const bf16*>(w), bias, cout, relu,
+                   static_cast<const bf16*>(mask), static_cast<bf16*>(y)};
+  const long long V = (long long)D * H * W;
+  const int gx = (int)((V + nnk::kBM - 1) / nnk::kBM);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int bn = cout % 64 == 0 ? 64 : (cout % 48 == 0 ? 48 : (cout % 32 == 0 ? 32 : 16));
+  const dim3 grid(gx, cout / bn);
+  clarity::note_launch_begin(clarity::KK_OTHER, st);
+  switch (bn) {
+    case 64: CLARITY_LAUNCH(nnk::k_conv3<64>, grid, 128, 0, st)(a); break;
+    case 48: CLARITY_LAUNCH(nnk::k_conv3<48>, grid, 128, 0, st)(a); break;
+    case 32: CLARITY_LAUNCH(nnk::k_conv3<32>, grid, 128, 0, st)(a); break;
+    default: CLARITY_LAUNCH(nnk::k_conv3<16>, grid, 128, 0, st)(a); break;
+  }
+  clarity::note_launch_end(clarity::KK_OTHER, st);
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_conv3_wgrad(const void* x1, int c1, const void* x2, int c2,
+                                                    int D, int H, int W, const void* dy, int cout,
+                                                    float* dw, float* dbias, void* stream) {
+  if (!x1 || !dy || !dw || D <= 0 || H <= 0 || W <= 0) return (ClarityResult_t)nn_bad("wgrad: argument");
+  if (c1 <= 0 || c1 % 16 || c2 < 0 || c2 % 16 || (c2 && !x2) || cout <= 0 || cout % 16)
+    return (ClarityResult_t)nn_bad("wgrad: channel counts must be multiples of 16");
+  if (c2 && (D % 2 || H % 2 || W % 2)) return (ClarityResult_t)nn_bad("wgrad: upsampled input needs even dims");
+  if (((uintptr_t)x1 | (uintptr_t)x2 | (uintptr_t)dy) & 15)
+    return (ClarityResult_t)nn_bad("wgrad: buffers must be 16-byte aligned");
+  nnk::Conv3Args a{static_cast<const bf16*>(x1), c1, static_cast<const bf16*>(x2), c2, D, H, W,
+                   D / 2, H / 2, W / 2, nullptr, nullptr, cout, 0, nullptr, nullptr};
+  const long long V = (long long)D * H * W;
+  const int cin = c1 + c2;
+  const int nblk = (27 * (cin / 16) + 3) / 4;
+  const int bm = cout % 64 == 0 ? 64 : (cout % 48 == 0 ? 48 : (cout % 32 == 0 ? 32 : 16));
+  const dim3 grid(nblk, cout / bm, (unsigned)((V + nnk::kVoxChunk - 1) / nnk::kVoxChunk));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bf16* d = static_cast<const bf16*>(dy);
+  clarity::note_launch_begin(clarity::KK_OTHER, st);
+  switch (bm) {
+    case 64: CLARITY_LAUNCH(nnk::k_conv3_wgrad<64>, grid, 128, 0, st)(a, d, dw); break;
+    case 48: CLARITY_LAUNCH(nnk::k_conv3_wgrad<48>, grid, 128, 0, st)(a, d, dw); break;
+    case 32: CLARITY_LAUNCH(nnk::k_conv3_wgrad<32>, grid, 128, 0, st)(a, d, dw); break;
+    default: CLARITY_LAUNCH(nnk::k_conv3_wgrad<16>, grid, 128, 0, st)(a, d, dw); break;
+  }
+  if (dbias)
+    CLARITY_LAUNCH(nnk::k_bias_grad, nnk::grid_for(V * cout), 256, cout * sizeof(float), st)(
+        d, V, cout, dbias);
+  clarity::note_launch_end(clarity::KK_OTHER, st);
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_conv_in(const float* x, int D, int H, int W, const float* w,
+                                                const float* b, void* y, void* stream) {
+  if (!x || !w || !b || !y || D <= 0 || H <= 0 || W <= 0) return (ClarityResult_t)nn_bad("conv_in: argument");
+  const long long V = (long long)D * H * W;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_conv_in, nnk::grid_for(V), 256, 0, st)(x, D, H, W, w, b,
+                                                               static_cast<bf16*>(y));
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_conv_in_wgrad(const float* x, int D, int H, int W,
+                                                      const void* dy, float* dw, float* db,
+                                                      void* stream) {
+  if (!x || !dy || !dw || !db || D <= 0 || H <= 0 || W <= 0) return (ClarityResult_t)nn_bad("conv_in_wgrad: argument");
+  const long long V = (long long)D * H * W;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_conv_in_wgrad, nnk::grid_for(V * 16), 256, 0, st)(
+      x, D, H, W, static_cast<const bf16*>(dy), dw, db);
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_head(const void* y, long long V, const float* w,
+                                             const float* b, float* r, void* stream) {
+  if (!y || !w || !b || !r || V <= 0) return (ClarityResult_t)nn_bad("head: argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_head, nnk::grid_for(V), 256, 0, st)(static_cast<const bf16*>(y), V, w, b, r);
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_head_loss_grad(const void* y, long long V, const float* w,
+                                                       const float* r, const float* t, void* dy,
+                                                       float* dw, float* db, double* loss,
+                                                       void* stream) {
+  if (!y || !w || !r || !t || !dy || !dw || !db || !loss || V <= 0)
+    return (ClarityResult_t)nn_bad("head_loss_grad: argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_head_loss_grad, nnk::grid_for(V), 256, 0, st)(
+      static_cast<const bf16*>(y), V, w, r, t, static_cast<bf16*>(dy), dw, db, loss);
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_pool2(const void* x, int C, int D, int H, int W, void* y,
+                                              void* stream) {
+  if (!x || !y || C <= 0 || D <= 0 || H <= 0 || W <= 0 || D % 2 || H % 2 || W % 2)
+    return (ClarityResult_t)nn_bad("pool2: argument (dims must be even)");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_pool2, nnk::grid_for((long long)D * H * W * C / 8), 256, 0, st)(
+      static_cast<const bf16*>(x), C, D, H, W, static_cast<bf16*>(y));
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_merge_skip_grad(const void* dxcat, int ccat,
+                                                        const void* dp, const void* s, int c,
+                                                        int D, int H, int W, void* out,
+                                                        void* stream) {
+  if (!s || !out || c <= 0 || D <= 0 || H <= 0 || W <= 0 || (dp && (D % 2 || H % 2 || W % 2)) ||
+      (dxcat && ccat < c))
+    return (ClarityResult_t)nn_bad("merge_skip_grad: argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_merge_skip_grad, nnk::grid_for((long long)D * H * W * c), 256, 0, st)(
+      static_cast<const bf16*>(dxcat), ccat, static_cast<const bf16*>(dp),
+      static_cast<const bf16*>(s), c, D, H, W, static_cast<bf16*>(out));
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_up_grad(const void* dxcat, int ccat, int c1, int c2,
+                                                const void* coarse, int D, int H, int W,
+                                                void* out, void* stream) {
+  if (!dxcat || !coarse || !out || c2 <= 0 || c1 < 0 || ccat != c1 + c2 || D % 2 || H % 2 ||
+      W % 2 || D <= 0 || H <= 0 || W <= 0)
+    return (ClarityResult_t)nn_bad("up_grad: argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_up_grad, nnk::grid_for((long long)D * H * W * c2 / 8), 256, 0, st)(
+      static_cast<const bf16*>(dxcat), ccat, c1, c2, static_cast<const bf16*>(coarse), D, H, W,
+      static_cast<bf16*>(out));
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_adam(float* p, const float* g, float* m, float* v,
+                                             long long n, float lr, float b1, float b2, float eps,
+                                             int step, void* stream) {
+  if (!p || !g || !m || !v || n <= 0 || step <= 0) return (ClarityResult_t)nn_bad("adam: argument");
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_adam, nnk::grid_for(n), 256, 0, st)(p, g, m, v, n, lr, b1, b2, eps, c1, c2);
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+CLARITY_API ClarityResult_t clarityx_nn_pack_weights(const float* w, int cout, int cin, void* wf,
+                                                     void* wb, void* stream) {
+  if (!w || !wf || cout <= 0 || cin <= 0) return (ClarityResult_t)nn_bad("pack_weights: argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CLARITY_LAUNCH(nnk::k_pack_weights, nnk::grid_for((long long)cout * 27 * cin), 256, 0, st)(
+      w, cout, cin, static_cast<bf16*>(wf), static_cast<bf16*>(wb));
+  return (ClarityResult_t)nn_err(cudaGetLastError());
+}
+
+}  // extern "C"

@@ -24,32 +24,37 @@ T* dynamic_smem() {
 }
 
 struct Launcher {
-  long long grid;
+  dim3 grid;
   size_t smem;
   template <class K>
   auto operator()(K kernel) const {
-    const long long g = grid;
+    const dim3 g = grid;
     const size_t s = smem;
     return [g, s, kernel](auto... args) {
-      for (long long b = 0; b < g; ++b) {
-        bIdx = make_uint3((unsigned)b, 0, 0);
-        tIdx = make_uint3(0, 0, 0);
-        bDim = dim3(1, 1, 1);
-        gDim = dim3((unsigned)g, 1, 1);
-        void* p = nullptr;
-        if (s) {
-          p = std::aligned_alloc(128, (s + 127) / 128 * 128);  // as __align__(128)
-          std::memset(p, 0xff, s);
-        }
-        smem_ptr = p;
-        kernel(args...);
-        std::free(p);
-        smem_ptr = nullptr;
-      }
+      for (unsigned bz = 0; bz < g.z; ++bz)
+        for (unsigned by = 0; by < g.y; ++by)
+          for (unsigned bx = 0; bx < g.x; ++bx) {
+            bIdx = make_uint3(bx, by, bz);
+            tIdx = make_uint3(0, 0, 0);
+            bDim = dim3(1, 1, 1);
+            gDim = g;
+            void* p = nullptr;
+            if (s) {
+              p = std::aligned_alloc(128, (s + 127) / 128 * 128);  // as __align__(128)
+              std::memset(p, 0xff, s);
+            }
+            smem_ptr = p;
+            kernel(args...);
+            std::free(p);
+            smem_ptr = nullptr;
+          }
     };
   }
 };
-inline Launcher launcher(long long grid, size_t smem) { return Launcher{grid, smem}; }
+inline Launcher launcher(long long grid, size_t smem) {
+  return Launcher{dim3((unsigned)grid, 1, 1), smem};
+}
+inline Launcher launcher(dim3 grid, size_t smem) { return Launcher{grid, smem}; }
 }  // namespace clarity_emu
 
 #ifndef __noinline__
@@ -72,6 +77,17 @@ inline T __ldg(const T* p) {
 inline float __shfl_xor_sync(unsigned, float, int) { return 0.f; }
 inline double __shfl_xor_sync(unsigned, double, int) { return 0.0; }
 inline void __syncthreads() {}
+// one thread per block: atomics are plain read-modify-writes
+inline float atomicAdd(float* p, float v) {
+  const float o = *p;
+  *p = o + v;
+  return o;
+}
+inline double atomicAdd(double* p, double v) {
+  const double o = *p;
+  *p = o + v;
+  return o;
+}
 inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline void sincospi(double x, double* s, double* c) {
   *s = std::sin(M_PI * x);
