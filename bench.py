@@ -195,6 +195,17 @@ NCU_TRAFFIC = {"xy_product": 152.1e6 + 215.3e6, "xy_inv_fwd": 84.5e6 + 19.4e6,
                "z": (271.7e6 + 88.3e6 + 203.6e6 + 86.2e6) / 2}
 
 
+def max_over_ranks(value, dist, device):
+    """The slowest rank's figure (replicas: every rank solves its own volume;
+    the job is done when the last one is).  `dist` None: one rank."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=60):
     """The second metric: device time until I-div(g, h*u) is within 1% of
     plain RL's value after `plain_iters` iterations, for plain RL and for the
@@ -306,7 +317,7 @@ def run_gpu_arm(args, rank, world):
     e1.record(stream)
     torch.cuda.synchronize()
     launches = api.launch_count() - l0
-    ms_total = e0.elapsed_time(e1)
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     # per-kernel-family durations: one more step, outside the timed region,
     # with CUDA events recorded around every fused-pass launch on its stream
     api.timing_enable(True)
@@ -315,9 +326,6 @@ def run_gpu_arm(args, rank, world):
     fam = api.timing_collect()
     api.timing_enable(False)
     if dist:
-        t = torch.tensor([ms_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
         dist.barrier()
     ms_step = ms_total / args.steps
     vox = int(np.prod(IMAGE_ZYX))
@@ -353,11 +361,7 @@ def run_gpu_arm(args, rank, world):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - t0) / args.steps, dist, "cuda")
     clk = clocks.stop()
     e2e_value = world * vox * ITERS / (e2e_ms / 1e3) / 1e9
 

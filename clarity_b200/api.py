@@ -57,6 +57,10 @@ EXTENSION_SYMBOLS = [
     "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
     "clarityx_convolve_noalloc", "clarityx_ml_batch_device", "clarityx_autotune",
     "clarityx_ml_ex_device", "clarityx_ml_accel_device",
+    "clarityx_nn_conv3", "clarityx_nn_conv3_wgrad", "clarityx_nn_conv_in",
+    "clarityx_nn_conv_in_wgrad", "clarityx_nn_head", "clarityx_nn_head_loss_grad",
+    "clarityx_nn_pool2", "clarityx_nn_merge_skip_grad", "clarityx_nn_up_grad",
+    "clarityx_nn_adam", "clarityx_nn_pack_weights",
 ]
 BATCH_GRAPH = 1  # CLARITYX_BATCH_GRAPH
 

@@ -129,6 +129,62 @@ CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, void *stream);
 
+/* Learned-start network kernels (clarity_b200/unet.py builds the network on
+ * them).  Device pointers; activations are BF16 [v][c] with v = (z*H + y)*W +
+ * x, weights BF16 [cout][27][cin] with tap = (dz+1)*9 + (dy+1)*3 + (dx+1),
+ * accumulation FP32.  Channel counts of conv3/conv3_wgrad are multiples of 16;
+ * buffers 16-byte aligned.  No reference counterpart.
+ *
+ * conv3: y = act(bias + 3x3x3 convolution, zero padding) of x1 [D,H,W,c1]
+ *   concatenated with x2 [D/2,H/2,W/2,c2] read through nearest upsampling (x2
+ *   may be NULL, c2 = 0); act = ReLU when relu, then y *= (mask > 0) when mask
+ *   is given.  Tensor cores (mma.sync bf16, FP32 accumulate).
+ * conv3_wgrad: dw[cout][27][cin] += sum_v dy[v][co] in(v + tap)[ci], dbias[co]
+ *   += sum_v dy[v][co] (FP32, accumulated: zero them first).
+ * conv_in / conv_in_wgrad: the 1 -> 16 first layer (float input, FP32
+ *   weights [16][27]), ReLU output.
+ * head / head_loss_grad: r = b + sum_c w[c] y[v][c] over 16 channels; the loss
+ *   mean (r - t)^2 added to *loss, its gradient dy (masked by y > 0), dw, db.
+ * pool2: 2x2x2 average pool.  merge_skip_grad: (dxcat[.., 0:c] + dp/8
+ *   upsampled) * (s > 0).  up_grad: 2x2x2 sums of dxcat[.., c1:c1+c2] masked by
+ *   coarse > 0.  adam: one bias-corrected Adam step.  pack_weights: BF16
+ *   forward weights and the mirrored, transposed backward-data weights from the
+ *   FP32 master copy. */
+CLARITY_API ClarityResult_t clarityx_nn_conv3(const void *x1, int c1, const void *x2, int c2,
+                                              int D, int H, int W, const void *w,
+                                              const float *bias, int cout, int relu,
+                                              const void *mask, void *y, void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_conv3_wgrad(const void *x1, int c1, const void *x2,
+                                                    int c2, int D, int H, int W, const void *dy,
+                                                    int cout, float *dw, float *dbias,
+                                                    void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_conv_in(const float *x, int D, int H, int W,
+                                                const float *w, const float *b, void *y,
+                                                void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_conv_in_wgrad(const float *x, int D, int H, int W,
+                                                      const void *dy, float *dw, float *db,
+                                                      void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_head(const void *y, long long V, const float *w,
+                                             const float *b, float *r, void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_head_loss_grad(const void *y, long long V,
+                                                       const float *w, const float *r,
+                                                       const float *t, void *dy, float *dw,
+                                                       float *db, double *loss, void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_pool2(const void *x, int C, int D, int H, int W,
+                                              void *y, void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_merge_skip_grad(const void *dxcat, int ccat,
+                                                        const void *dp, const void *s, int c,
+                                                        int D, int H, int W, void *out,
+                                                        void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_up_grad(const void *dxcat, int ccat, int c1, int c2,
+                                                const void *coarse, int D, int H, int W,
+                                                void *out, void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_adam(float *p, const float *g, float *m, float *v,
+                                             long long n, float lr, float b1, float b2,
+                                             float eps, int step, void *stream);
+CLARITY_API ClarityResult_t clarityx_nn_pack_weights(const float *w, int cout, int cin,
+                                                     void *wf, void *wb, void *stream);
+
 /* Benchmark probes.  clarityx_launch_count: kernels the library has
  * launched so far.  clarityx_timing_enable(1) makes every fused-pass launch
  * record a CUDA event pair on its stream; clarityx_timing_collect waits for

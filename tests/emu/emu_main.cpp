@@ -2,11 +2,14 @@
 // the CPU emulation build.
 //   emu_main <op> ix iy iz kx ky kz <param> image.raw psf.raw out.raw
 // op: convolve | rl | blind | jvc | sjvc | wiener (param = iterations or epsilon).
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
+
+#include <cuda_bf16.h>
 
 #include "../../include/clarity.h"
 #include "../../include/clarity_ext.h"
@@ -22,6 +25,58 @@ static std::vector<float> read_raw(const char* path, size_t n) {
   return v;
 }
 
+// Learned-start convolution kernels on deterministic BF16 data: dims (W, H,
+// D) = id, channels (c1, c2, cout) = kd.  Writes the inputs and results as
+// float32 files prefix.{x1,x2,w,b,dy,y,dx,dw,db} for the test to check.
+static float hval(uint32_t i, float scale) {
+  const uint32_t h = i * 2654435761u + 12345u;
+  return scale * ((float)((h >> 8) % 2001) / 1000.0f - 1.0f);
+}
+static void dump(const std::string& path, const std::vector<float>& v) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  std::fwrite(v.data(), sizeof(float), v.size(), f);
+  std::fclose(f);
+}
+static int nn_conv_case(Clarity_Dim3 id, Clarity_Dim3 kd, int relu, const char* prefix) {
+  const int W = id.x, H = id.y, D = id.z, c1 = kd.x, c2 = kd.y, co = kd.z, cin = c1 + c2;
+  const size_t V = (size_t)D * H * W, V2 = c2 ? V / 8 : 0;
+  auto mk = [](size_t n, uint32_t seed, float scale, std::vector<__nv_bfloat16>* b,
+               std::vector<float>* f) {
+    b->resize(n);
+    f->resize(n);
+    for (size_t i = 0; i < n; ++i) {
+      (*b)[i] = __float2bfloat16_rn(hval((uint32_t)i * 7u + seed, scale));
+      (*f)[i] = __bfloat162float((*b)[i]);
+    }
+  };
+  std::vector<__nv_bfloat16> x1, x2, wq, dy, y(V * co), dx(V * cin);
+  std::vector<float> fx1, fx2, fw, fdy, fb(co);
+  mk(V * c1, 1, 1.0f, &x1, &fx1);
+  mk(V2 * c2, 2, 1.0f, &x2, &fx2);
+  mk((size_t)co * 27 * cin, 3, 0.1f, &wq, &fw);
+  mk(V * co, 4, 1.0f, &dy, &fdy);
+  for (int i = 0; i < co; ++i) fb[i] = hval(100 + i, 0.2f);
+  ClarityResult_t r = clarityx_nn_conv3(x1.data(), c1, c2 ? x2.data() : nullptr, c2, D, H, W,
+                                        wq.data(), fb.data(), co, relu, nullptr, y.data(), nullptr);
+  if (r != CLARITY_SUCCESS) return 4;
+  std::vector<float> dw((size_t)co * 27 * cin, 0.f), db(co, 0.f);
+  r = clarityx_nn_conv3_wgrad(x1.data(), c1, c2 ? x2.data() : nullptr, c2, D, H, W, dy.data(), co,
+                              dw.data(), db.data(), nullptr);
+  if (r != CLARITY_SUCCESS) return 4;
+  std::vector<float> fy(y.size());
+  for (size_t i = 0; i < y.size(); ++i) fy[i] = __bfloat162float(y[i]);
+  const std::string p = prefix;
+  dump(p + ".x1", fx1);
+  dump(p + ".x2", fx2);
+  dump(p + ".w", fw);
+  dump(p + ".b", fb);
+  dump(p + ".dy", fdy);
+  dump(p + ".y", fy);
+  dump(p + ".dw", dw);
+  dump(p + ".db", db);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc != 12) {
     std::fprintf(stderr, "usage: emu_main op ix iy iz kx ky kz param img psf out\n");
@@ -31,6 +86,7 @@ int main(int argc, char** argv) {
   Clarity_Dim3 id{std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4])};
   Clarity_Dim3 kd{std::atoi(argv[5]), std::atoi(argv[6]), std::atoi(argv[7])};
   const double param = std::atof(argv[8]);
+  if (op == "nnconv") return nn_conv_case(id, kd, (int)param, argv[11]);
   const size_t ni = (size_t)id.x * id.y * id.z, nk = (size_t)kd.x * kd.y * kd.z;
   std::vector<float> img = read_raw(argv[9], ni), psf = read_raw(argv[10], nk), out(ni);
   if (Clarity_Register() != CLARITY_SUCCESS) return 3;

@@ -102,3 +102,35 @@ def test_emulated_library_matches_oracle(emu, tmp_path, oracle_lib, img_zyx, psf
     # emu_main), the first against the oracle
     assert rel_l2(run_emu(emu, tmp_path, "batch", img, psf, 2),
                   oracle_lib.rl(img, psf, 2)) <= 2e-6
+
+
+@pytest.mark.parametrize("dims,chans", [((8, 6, 10), (16, 0, 16)), ((4, 6, 8), (16, 32, 48)),
+                                        ((6, 4, 6), (32, 0, 64))])
+def test_emulated_nn_conv3_matches_reference(emu, tmp_path, dims, chans):
+    # the learned-start convolution kernels' tiles and index arithmetic (the
+    # tensor-core fragments are replaced by scalar loops over the same shared
+    # memory tiles) against the FP64 reference
+    torch = pytest.importorskip("torch")
+    import nn_ref as R
+    D, H, W = dims
+    c1, c2, co = chans
+    pre = str(tmp_path / "nn")
+    p = subprocess.run([emu, "nnconv", str(W), str(H), str(D), str(c1), str(c2), str(co), "1",
+                        "-", "-", pre], capture_output=True, text=True,
+                       env=dict(os.environ, ASAN_OPTIONS="detect_leaks=0"))
+    assert p.returncode == 0, p.stderr[-2000:]
+    rd = lambda s, shape: torch.from_numpy(np.fromfile(pre + "." + s, np.float32)
+                                           .reshape(shape).astype(np.float64))
+    cin = c1 + c2
+    x1 = rd("x1", (D, H, W, c1)).requires_grad_(True)
+    x2 = rd("x2", (D // 2, H // 2, W // 2, c2)) if c2 else None
+    w = rd("w", (co, 27, cin)).requires_grad_(True)
+    b = rd("b", (co,))
+    dy = rd("dy", (D, H, W, co))
+    ref = R.conv3(x1, w, co, bias=b, relu=False, x2=x2)
+    y = rd("y", (D, H, W, co))
+    assert (y - torch.relu(ref)).abs().max() <= 1e-2 * torch.relu(ref).abs().max()
+    (ref * dy).sum().backward()
+    dw = rd("dw", (co, 27, cin))
+    assert (dw - w.grad).abs().max() <= 1e-4 * w.grad.abs().max()
+    assert (rd("db", (co,)) - dy.sum(dim=(0, 1, 2))).abs().max() <= 1e-4 * dy.abs().sum()
