@@ -109,45 +109,65 @@ inline void cp_wait() {}
 #endif
 
 // out[v][co] = sum_{tap, c} in(v + tap)[c] w[co][tap][c] (+ bias, ReLU / mask).
-// Grid (ceil(V / 128), cout / BN), 128 threads; warp w owns voxel rows
-// [32w, 32w + 32) and all BN channels of the block.
+// One block computes a 2x8x8 (z, y, x) tile of output voxels for BN output
+// channels.  Per 16-channel input chunk it stages the tile's 4x10x10 halo
+// and all 27 taps' weights in shared memory once; the 27 tap GEMMs then read
+// their A rows from the halo at shifted positions (each lane of ldmatrix
+// supplies its own row address), so an input voxel is read from HBM/L2 once
+// per chunk instead of once per tap.  128 threads; warp w owns tile voxels
+// [32w, 32w + 32) (tile z = w / 2, y rows 4(w % 2) .. +3).
+constexpr int kTZ = 2, kTY = 8, kTX = 8;
+constexpr int kHZ = kTZ + 2, kHY = kTY + 2, kHX = kTX + 2;
+constexpr int kHalo = kHZ * kHY * kHX;  // 400 voxels
+
+template <int BN>
+struct Conv3Smem {
+  static constexpr int HALO = kHalo * kRow;     // bf16 elements
+  static constexpr int WTS = 27 * BN * kRow;
+  static constexpr int BYTES = (HALO + WTS) * 2;
+};
+
 template <int BN>
 __global__ void __launch_bounds__(128) k_conv3(const Conv3Args a) {
   static_assert(BN % 16 == 0 && BN <= 64, "BN: 16, 32, 48 or 64");
-  __shared__ alignas(128) bf16 As[2][kBM * kRow];
-  __shared__ alignas(128) bf16 Bs[2][BN * kRow];
+  CLARITY_DYN_SMEM(bf16, sm);
+  bf16* Hs = sm;                              // [halo voxel][24]
+  bf16* Ws = sm + Conv3Smem<BN>::HALO;        // [tap][n][24]
   const int cin = a.c1 + a.c2;
-  const int nsteps = 27 * (cin / 16);
-  const long long V = (long long)a.D * a.H * a.W;
-  const long long v0 = (long long)blockIdx.x * kBM;
+  const int nchunks = cin / 16;
+  const int ntx = (a.W + kTX - 1) / kTX, nty = (a.H + kTY - 1) / kTY;
+  const int tile = blockIdx.x;
+  const int tx0 = (tile % ntx) * kTX;
+  const int ty0 = ((tile / ntx) % nty) * kTY;
+  const int tz0 = (tile / (ntx * nty)) * kTZ;
   const int co0 = blockIdx.y * BN;
 
-  auto load = [&](int s, int stage) {
-    const int t = s / (cin / 16), cc = s - t * (cin / 16);
-    int dz, dy, dx;
-    tap_offset(t, &dz, &dy, &dx);
-    for (int q = threadIdx.x; q < 2 * kBM; q += CLARITY_BLOCK_STRIDE(128)) {
-      const int r = q >> 1, half = q & 1;
-      const long long v = v0 + r;
-      const bf16* src = nullptr;
-      if (v < V) {
-        const int x = (int)(v % a.W);
-        const long long zy = v / a.W;
-        const int y = (int)(zy % a.H), z = (int)(zy / a.H);
-        src = in_chunk(a, z + dz, y + dy, x + dx, cc * 16 + half * 8);
-      }
-      cp16(&As[stage][r * kRow + half * 8], src, a.x1);
+  auto load = [&](int cc) {
+    for (int q = threadIdx.x; q < 2 * kHalo; q += CLARITY_BLOCK_STRIDE(128)) {
+      const int h = q >> 1, half = q & 1;
+      const int hx = h % kHX, hy = (h / kHX) % kHY, hz = h / (kHX * kHY);
+      const bf16* src = in_chunk(a, tz0 - 1 + hz, ty0 - 1 + hy, tx0 - 1 + hx, cc * 16 + half * 8);
+      cp16(&Hs[h * kRow + half * 8], src, a.x1);
     }
-    for (int q = threadIdx.x; q < 2 * BN; q += CLARITY_BLOCK_STRIDE(128)) {
-      const int n = q >> 1, half = q & 1;
+    for (int q = threadIdx.x; q < 27 * BN * 2; q += CLARITY_BLOCK_STRIDE(128)) {
+      const int half = q & 1, tn = q >> 1;
+      const int n = tn % BN, t = tn / BN;
       const bf16* src = a.w + ((size_t)(co0 + n) * 27 + t) * cin + cc * 16 + half * 8;
-      cp16(&Bs[stage][n * kRow + half * 8], src, a.x1);
+      cp16(&Ws[(t * BN + n) * kRow + half * 8], src, a.x1);
     }
     cp_commit();
   };
 
 #ifndef CLARITY_HOST_EMULATION
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // halo index of this lane's A row for m tile i, at tap offset 0
+  int hrow[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int m = warp * 32 + i * 16 + (lane & 15);
+    const int tx = m % kTX, ty = (m / kTX) % kTY, tz = m / (kTX * kTY);
+    hrow[i] = ((tz + 1) * kHY + (ty + 1)) * kHX + (tx + 1);
+  }
   float acc[2][BN / 8][4];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
@@ -155,42 +175,43 @@ __global__ void __launch_bounds__(128) k_conv3(const Conv3Args a) {
     for (int j = 0; j < BN / 8; ++j)
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
-  load(0, 0);
-  for (int s = 0; s < nsteps; ++s) {
-    const int st = s & 1;
-    if (s + 1 < nsteps) {
-      load(s + 1, st ^ 1);
-      cp_wait<1>();
-    } else {
-      cp_wait<0>();
-    }
+  for (int cc = 0; cc < nchunks; ++cc) {
+    load(cc);
+    cp_wait<0>();
     __syncthreads();
-    uint32_t af[2][4];
+#pragma unroll 1
+    for (int t = 0; t < 27; ++t) {
+      const int toff = ((t / 9 - 1) * kHY + ((t / 3) % 3 - 1)) * kHX + (t % 3 - 1);
+      uint32_t af[2][4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-      ldm_x4(af[i], &As[st][(warp * 32 + i * 16 + (lane & 15)) * kRow + (lane >> 4) * 8]);
+      for (int i = 0; i < 2; ++i)
+        ldm_x4(af[i], &Hs[(hrow[i] + toff) * kRow + (lane >> 4) * 8]);
+      const bf16* wt = Ws + t * BN * kRow;
 #pragma unroll
-    for (int j = 0; j < BN / 8; j += 2) {
-      uint32_t bfr[4];
-      ldm_x4(bfr, &Bs[st][(j * 8 + (lane & 7) + (lane >> 4) * 8) * kRow + ((lane >> 3) & 1) * 8]);
+      for (int j = 0; j < BN / 8; j += 2) {
+        uint32_t bfr[4];
+        ldm_x4(bfr, &wt[(j * 8 + (lane & 7) + (lane >> 4) * 8) * kRow + ((lane >> 3) & 1) * 8]);
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        mma16816(acc[i][j], af[i], bfr);
-        mma16816(acc[i][j + 1], af[i], bfr + 2);
+        for (int i = 0; i < 2; ++i) {
+          mma16816(acc[i][j], af[i], bfr);
+          mma16816(acc[i][j + 1], af[i], bfr + 2);
+        }
       }
     }
     __syncthreads();
   }
-  // epilogue: acc[i][j] holds rows g, g+8 (g = lane/4) and columns 2(lane%4), +1
+  // epilogue: acc[i][j] holds tile rows g, g+8 (g = lane/4) and channels 2(lane%4), +1
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < BN / 8; ++j)
+    for (int h = 0; h < 2; ++h) {
+      const int m = warp * 32 + i * 16 + (lane >> 2) + h * 8;
+      const int x = tx0 + m % kTX, y = ty0 + (m / kTX) % kTY, z = tz0 + m / (kTX * kTY);
+      if (x >= a.W || y >= a.H || z >= a.D) continue;
+      const long long v = ((long long)z * a.H + y) * a.W + x;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const long long v = v0 + warp * 32 + i * 16 + (lane >> 2) + h * 8;
+      for (int j = 0; j < BN / 8; ++j) {
         const int co = co0 + j * 8 + (lane & 3) * 2;
-        if (v >= V) continue;
         float r0 = acc[i][j][2 * h], r1 = acc[i][j][2 * h + 1];
         if (a.bias) {
           r0 += a.bias[co];
@@ -202,38 +223,47 @@ __global__ void __launch_bounds__(128) k_conv3(const Conv3Args a) {
         }
         const size_t o = (size_t)v * a.cout + co;
         if (a.mask) {
-          const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162*>(a.mask + o);
-          if (!(__bfloat162float(m.x) > 0.f)) r0 = 0.f;
-          if (!(__bfloat162float(m.y) > 0.f)) r1 = 0.f;
+          const __nv_bfloat162 mk = *reinterpret_cast<const __nv_bfloat162*>(a.mask + o);
+          if (!(__bfloat162float(mk.x) > 0.f)) r0 = 0.f;
+          if (!(__bfloat162float(mk.y) > 0.f)) r1 = 0.f;
         }
         *reinterpret_cast<__nv_bfloat162*>(a.y + o) = __floats2bfloat162_rn(r0, r1);
       }
+    }
 #else
   // host emulation: the same tiles, multiplied with scalar loops
-  static thread_local float accs[kBM][64];
-  for (int r = 0; r < kBM; ++r)
+  static thread_local float accs[kTZ * kTY * kTX][64];
+  for (int r = 0; r < 128; ++r)
     for (int n = 0; n < BN; ++n) accs[r][n] = 0.f;
-  for (int s = 0; s < nsteps; ++s) {
-    load(s, 0);
-    for (int r = 0; r < kBM; ++r)
-      for (int n = 0; n < BN; ++n) {
-        float t = 0.f;
-        for (int k = 0; k < 16; ++k)
-          t += __bfloat162float(As[0][r * kRow + k]) * __bfloat162float(Bs[0][n * kRow + k]);
-        accs[r][n] += t;
+  for (int cc = 0; cc < nchunks; ++cc) {
+    load(cc);
+    for (int t = 0; t < 27; ++t) {
+      const int toff = ((t / 9 - 1) * kHY + ((t / 3) % 3 - 1)) * kHX + (t % 3 - 1);
+      for (int m = 0; m < 128; ++m) {
+        const int tx = m % kTX, ty = (m / kTX) % kTY, tz = m / (kTX * kTY);
+        const int hr = ((tz + 1) * kHY + (ty + 1)) * kHX + (tx + 1) + toff;
+        for (int n = 0; n < BN; ++n) {
+          float acc1 = 0.f;
+          for (int k = 0; k < 16; ++k)
+            acc1 += __bfloat162float(Hs[hr * kRow + k]) *
+                    __bfloat162float(Ws[(t * BN + n) * kRow + k]);
+          accs[m][n] += acc1;
+        }
       }
+    }
   }
-  for (int r = 0; r < kBM; ++r) {
-    const long long v = v0 + r;
-    if (v >= V) continue;
+  for (int m = 0; m < 128; ++m) {
+    const int x = tx0 + m % kTX, y = ty0 + (m / kTX) % kTY, z = tz0 + m / (kTX * kTY);
+    if (x >= a.W || y >= a.H || z >= a.D) continue;
+    const long long v = ((long long)z * a.H + y) * a.W + x;
     for (int n = 0; n < BN; ++n) {
       const int co = co0 + n;
-      float x = accs[r][n];
-      if (a.bias) x += a.bias[co];
-      if (a.relu) x = fmaxf(x, 0.f);
+      float xv = accs[m][n];
+      if (a.bias) xv += a.bias[co];
+      if (a.relu) xv = fmaxf(xv, 0.f);
       const size_t o = (size_t)v * a.cout + co;
-      if (a.mask && !(__bfloat162float(a.mask[o]) > 0.f)) x = 0.f;
-      a.y[o] = __float2bfloat16_rn(x);
+      if (a.mask && !(__bfloat162float(a.mask[o]) > 0.f)) xv = 0.f;
+      a.y[o] = __float2bfloat16_rn(xv);
     }
   }
 #endif
@@ -630,19 +660,31 @@ CLARITY_API ClarityResult_t clarityx_nn_conv3(const void* x1, int c1, const void
   nnk::Conv3Args a{static_cast<const bf16*>(x1), c1, static_cast<const bf16*>(x2), c2, D, H, W,
                    D / 2, H / 2, W / 2, static_cast<const bf16*>(w), bias, cout, relu,
                    static_cast<const bf16*>(mask), static_cast<bf16*>(y)};
-  const long long V = (long long)D * H * W;
-  const int gx = (int)((V + nnk::kBM - 1) / nnk::kBM);
+  const long long tiles = (long long)((D + nnk::kTZ - 1) / nnk::kTZ) *
+                          ((H + nnk::kTY - 1) / nnk::kTY) * ((W + nnk::kTX - 1) / nnk::kTX);
+  if (tiles > 0x7fffffffll) return (ClarityResult_t)nn_bad("conv3: volume too large");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int bn = cout % 64 == 0 ? 64 : (cout % 48 == 0 ? 48 : (cout % 32 == 0 ? 32 : 16));
-  const dim3 grid(gx, cout / bn);
+  // output channels per block: 48 KB-class shared memory (halo + 27 taps)
+  const int bn = cout % 48 == 0 ? 48 : (cout % 32 == 0 ? 32 : 16);
+  const dim3 grid((unsigned)tiles, cout / bn);
   clarity::note_launch_begin(clarity::KK_OTHER, st);
+  cudaError_t e = cudaSuccess;
   switch (bn) {
-    case 64: CLARITY_LAUNCH(nnk::k_conv3<64>, grid, 128, 0, st)(a); break;
-    case 48: CLARITY_LAUNCH(nnk::k_conv3<48>, grid, 128, 0, st)(a); break;
-    case 32: CLARITY_LAUNCH(nnk::k_conv3<32>, grid, 128, 0, st)(a); break;
-    default: CLARITY_LAUNCH(nnk::k_conv3<16>, grid, 128, 0, st)(a); break;
+    case 48:
+      e = clarity::smem_opt_in(reinterpret_cast<const void*>(nnk::k_conv3<48>), nnk::Conv3Smem<48>::BYTES);
+      if (e == cudaSuccess) CLARITY_LAUNCH(nnk::k_conv3<48>, grid, 128, nnk::Conv3Smem<48>::BYTES, st)(a);
+      break;
+    case 32:
+      e = clarity::smem_opt_in(reinterpret_cast<const void*>(nnk::k_conv3<32>), nnk::Conv3Smem<32>::BYTES);
+      if (e == cudaSuccess) CLARITY_LAUNCH(nnk::k_conv3<32>, grid, 128, nnk::Conv3Smem<32>::BYTES, st)(a);
+      break;
+    default:
+      e = clarity::smem_opt_in(reinterpret_cast<const void*>(nnk::k_conv3<16>), nnk::Conv3Smem<16>::BYTES);
+      if (e == cudaSuccess) CLARITY_LAUNCH(nnk::k_conv3<16>, grid, 128, nnk::Conv3Smem<16>::BYTES, st)(a);
+      break;
   }
   clarity::note_launch_end(clarity::KK_OTHER, st);
+  if (e != cudaSuccess) return (ClarityResult_t)nn_err(e);
   return (ClarityResult_t)nn_err(cudaGetLastError());
 }
 
