@@ -254,26 +254,30 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
         res["chosen"]["idiv"] = finals[k_acc]
         res["speedup"] = res["plain"]["ms"] / res["chosen"]["ms"]
     # learned start (when trained weights are present): RL 5 iterations, the
-    # network's prediction, RL resumed from it until the target is met
+    # network's prediction, RL resumed from it (plain or accelerated) until
+    # the target is met
     from clarity_b200 import learned
     if os.path.exists(learned.WEIGHTS):
         net = learned.load_net()
-        k_ls, ls_final = None, None
-        for k in range(1, max_accel + 1):
-            tl = torch.zeros(k + 1, dtype=torch.float64, device="cuda")
-            learned.learned_solve(net, img_d, psf_d, out, k, idiv=tl, stream=stream)
-            torch.cuda.synchronize()
-            if float(tl[k].item()) <= target:
-                k_ls, ls_final = k, float(tl[k].item())
-                break
-        ls = {"form": "learned start (3-D U-Net on RL iterate 5, BF16 tensor-core kernels) "
-                      "+ resumed RL", "pre_iterations": 5, "resumed_iterations": k_ls}
-        if k_ls:
-            ls["ms"] = ev_ms(lambda: learned.learned_solve(net, img_d, psf_d, out, k_ls,
-                                                           stream=stream))
-            ls["idiv"] = ls_final
-            ls["speedup"] = res["plain"]["ms"] / ls["ms"]
-        res["learned_start"] = ls
+        for tag, accel in (("learned_start", False), ("learned_start_accel", True)):
+            k_ls, ls_final = None, None
+            for k in range(1, max_accel + 1):
+                tl = torch.zeros(k + 1, dtype=torch.float64, device="cuda")
+                learned.learned_solve(net, img_d, psf_d, out, k, idiv=tl, stream=stream,
+                                      accel=accel)
+                torch.cuda.synchronize()
+                if float(tl[k].item()) <= target:
+                    k_ls, ls_final = k, float(tl[k].item())
+                    break
+            ls = {"form": "learned start (3-D U-Net on RL iterate 5, BF16 tensor-core kernels) "
+                          + ("+ accelerated RL" if accel else "+ resumed RL"),
+                  "pre_iterations": 5, "resumed_iterations": k_ls}
+            if k_ls:
+                ls["ms"] = ev_ms(lambda: learned.learned_solve(net, img_d, psf_d, out, k_ls,
+                                                               stream=stream, accel=accel))
+                ls["idiv"] = ls_final
+                ls["speedup"] = res["plain"]["ms"] / ls["ms"]
+            res[tag] = ls
     return res
 
 

@@ -149,7 +149,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_ml_batch_device.restype = i
         L.clarityx_ml_ex_device.argtypes = [vp, Dim3, vp, Dim3, vp, vp, i, vp, vp]
         L.clarityx_ml_ex_device.restype = i
-        L.clarityx_ml_accel_device.argtypes = [vp, Dim3, vp, Dim3, vp, i, vp, vp]
+        L.clarityx_ml_accel_device.argtypes = [vp, Dim3, vp, Dim3, vp, vp, i, vp, vp]
         L.clarityx_ml_accel_device.restype = i
         L.clarityx_autotune.argtypes = [i]
         L.clarityx_autotune.restype = None
@@ -417,10 +417,13 @@ def ml_ex_device(image, kernel, out, iterations, start=None, idiv=None, stream=N
     return out
 
 
-def ml_accel_device(image, kernel, out, iterations, idiv=None, stream=None):
+def ml_accel_device(image, kernel, out, iterations, idiv=None, stream=None, start=None):
     """clarityx_ml_accel_device: accelerated RL (Biggs-Andrews extrapolation)
-    with an optional I-divergence trace (`iterations` + 1 float64 entries)."""
-    for t in (image, kernel, out):
+    from `start` (None: the image) with an optional I-divergence trace
+    (`iterations` + 1 float64 entries)."""
+    if start is not None and tuple(start.shape) != tuple(image.shape):
+        raise ValueError("start must have the image's shape")
+    for t in (image, kernel, out) + ((start,) if start is not None else ()):
         if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
             raise ValueError("device variants need contiguous float32 CUDA tensors")
     if idiv is not None and not (idiv.is_cuda and str(idiv.dtype) == "torch.float64"
@@ -429,6 +432,7 @@ def ml_accel_device(image, kernel, out, iterations, idiv=None, stream=None):
     vp = C.c_void_p
     _check(load().clarityx_ml_accel_device(
         vp(image.data_ptr()), dim3(image), vp(kernel.data_ptr()), dim3(kernel),
+        vp(start.data_ptr()) if start is not None else None,
         vp(out.data_ptr()), int(iterations), vp(idiv.data_ptr()) if idiv is not None else None,
         _stream_ptr(stream)))
     return out

@@ -420,12 +420,13 @@ ClarityResult_t clarityx_ml_ex_device(const float* image, Clarity_Dim3 imageDim,
 }
 
 ClarityResult_t clarityx_ml_accel_device(const float* image, Clarity_Dim3 imageDim,
-                                         const float* kernel, Clarity_Dim3 kernelDim, float* out,
-                                         int iterations, double* idiv, void* stream) {
+                                         const float* kernel, Clarity_Dim3 kernelDim,
+                                         const float* start, float* out, int iterations,
+                                         double* idiv, void* stream) {
   return device_call(image, imageDim, kernel, kernelDim, out, stream,
                      [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
                          float* o) {
-                       return clarity::run_rl_accel(c, i, id, k, kd, o, iterations, idiv);
+                       return clarity::run_rl_accel(c, i, id, k, kd, start, o, iterations, idiv);
                      });
 }
 

@@ -919,7 +919,7 @@ Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims
 // The three estimate buffers rotate (x_prev, x, x_next); idiv as run_rl_ex,
 // its entries k < iters taken at y_k.
 Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
-                    float* out, int iters, double* idiv) {
+                    const float* start, float* out, int iters, double* idiv) {
   const PlanEntry* pe;
   Workspace* ws;
   Dims wd;
@@ -927,7 +927,7 @@ Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, D
   cudaStream_t st = ctx.exec_stream();
   if (iters <= 0) {
     count_small();
-    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, st)(img, out, id.n());
+    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, st)(start ? start : img, out, id.n());
     CL_CHECK(cudaGetLastError());
     return Status::Ok();
   }
@@ -961,7 +961,8 @@ Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, D
   int xi = 0, pi = 0, ui = 1;  // x, x_prev, x_next buffers (x_prev = x at first)
   CL_TRY(reduce_sum_into(ctx, img, id.n(), ws->partial, ws->dscal + 0));
   count_small();
-  CLARITY_LAUNCH(k_pad_image, kReduceBlocks, 256, 0, st)(g, wv, B[0]);
+  CLARITY_LAUNCH(k_pad_image, kReduceBlocks, 256, 0, st)(start ? image_src(start, id) : g, wv,
+                                                         B[0]);
   CL_CHECK(cudaMemsetAsync(alpha, 0, sizeof(float), st));
   for (int k = 0; k < iters; ++k) {
     CL_TRY(xy_forward(ctx, *pe, ProAccel{B[xi], B[pi], alpha, Y, wv, P.xmode}, ws->S));

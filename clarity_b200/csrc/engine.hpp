@@ -134,11 +134,11 @@ Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
 // the image against h * the estimate at the start of each iteration).
 Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
                  const float* start, float* out, int iters, double* idiv);
-// Accelerated Richardson-Lucy (Biggs-Andrews vector extrapolation), optional
-// I-divergence trace as run_rl_ex (entries k < iters at the extrapolated
-// points).
+// Accelerated Richardson-Lucy (Biggs-Andrews vector extrapolation) from
+// `start` (image-sized; nullptr: the image), optional I-divergence trace as
+// run_rl_ex (entries k < iters at the extrapolated points).
 Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
-                    float* out, int iters, double* idiv);
+                    const float* start, float* out, int iters, double* idiv);
 // Richardson-Lucy on n independent volumes of any sizes (device pointers):
 // each volume has its own plan and workspace, volumes run concurrently on the
 // batch stream pool, and with use_graph the whole batch is captured into one

@@ -105,9 +105,10 @@ def train(net: unet.UNet3D, xe, xl, epochs: int = 6, lr: float = 1e-3, batch: in
 
 
 def learned_solve(net: unet.UNet3D, img_d, psf_d, out, post: int, pre: int = 5,
-                  idiv=None, stream=None):
+                  idiv=None, stream=None, accel=False):
     """RL `pre` iterations, the network's prediction, RL resumed for `post`
-    iterations from it (idiv: trace of the resumed part, post + 1 entries)."""
+    iterations from it -- plain, or accelerated (Biggs-Andrews) with accel
+    (idiv: trace of the resumed part, post + 1 entries)."""
     import torch
     early = torch.empty_like(img_d)
     api.ml_device(img_d, psf_d, early, pre, stream)
@@ -115,7 +116,10 @@ def learned_solve(net: unet.UNet3D, img_d, psf_d, out, post: int, pre: int = 5,
     if post <= 0:
         out.copy_(start)
         return out
-    api.ml_ex_device(img_d, psf_d, out, post, start=start, idiv=idiv, stream=stream)
+    if accel:
+        api.ml_accel_device(img_d, psf_d, out, post, idiv=idiv, stream=stream, start=start)
+    else:
+        api.ml_ex_device(img_d, psf_d, out, post, start=start, idiv=idiv, stream=stream)
     return out
 
 

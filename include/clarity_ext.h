@@ -59,12 +59,12 @@ CLARITY_API ClarityResult_t clarityx_ml_ex_device(
  * Clarity_MaximumLikelihoodDeconvolve applied at extrapolated points
  * y = max(0, x + alpha (x - x_prev)), alpha from the last two steps (vector
  * extrapolation of Biggs and Andrews, Applied Optics 36(8):1766-1775, 1997).
- * No reference counterpart.  idiv as clarityx_ml_ex_device (entries before the
- * last taken at the extrapolated points). */
+ * No reference counterpart.  start and idiv as clarityx_ml_ex_device (trace
+ * entries before the last taken at the extrapolated points). */
 CLARITY_API ClarityResult_t clarityx_ml_accel_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
-    Clarity_Dim3 kernelDim, float *out, int iterations, double *idiv,
-    void *stream);
+    Clarity_Dim3 kernelDim, const float *start, float *out, int iterations,
+    double *idiv, void *stream);
 
 /* Richardson-Lucy on `count` independent volumes of any sizes (device
  * pointers, one kernel per volume): each volume has its own plan and

@@ -106,8 +106,8 @@ int main(int argc, char** argv) {
     r = Clarity_SmoothedJansenVanCittertDeconvolve(img.data(), id, psf.data(), kd, out.data(),
                                                    (unsigned)param, 2u, sig);
   } else if (op == "accel") {  // accelerated RL, emulated device memory is host memory
-    r = clarityx_ml_accel_device(img.data(), id, psf.data(), kd, out.data(), (int)param, nullptr,
-                                 nullptr);
+    r = clarityx_ml_accel_device(img.data(), id, psf.data(), kd, nullptr, out.data(), (int)param,
+                                 nullptr, nullptr);
   } else if (op == "batch") {
     // three volumes of different sizes in one batched call (emulated device
     // memory is host memory); each must equal its single-volume solve
