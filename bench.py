@@ -281,6 +281,56 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
     return res
 
 
+def _cfg2_case(i):
+    from clarity_b200 import synthetic as syn
+    img, psf, _ = syn.cfg2_volume(i)
+    return img, psf
+
+
+def other_configs(api, torch, stream, n_batch=64, batch_iters=30, cfg3_iters=10):
+    """The batched and the large-volume workloads, measured beside the headline
+    (G image-voxel-iterations/s; CUDA events on the launching stream)."""
+    import multiprocessing as mp
+    from clarity_b200 import synthetic as syn
+    res = {}
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 4)) as pool:
+        cases = pool.map(_cfg2_case, range(n_batch))
+    imgs = [torch.from_numpy(a).cuda() for a, _ in cases]
+    psfs = [torch.from_numpy(b).cuda() for _, b in cases]
+    outs = [torch.empty_like(a) for a in imgs]
+    vox = sum(a.numel() for a in imgs)
+    api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)  # set-up+capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 3
+    res["batched_rl"] = {"workload": f"{n_batch} volumes of uneven sizes (x, y in 16*{{6..20}}, "
+                                     f"z in 8*{{2..12}}), {batch_iters} RL iterations, one "
+                                     "captured CUDA graph", "image_voxels": int(vox),
+                         "ms": ms, "value": vox * batch_iters / (ms / 1e3) / 1e9,
+                         "unit": "Gvoxel-iter/s"}
+    del imgs, psfs, outs
+    img, psf, _ = syn.cfg3()
+    di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
+    out = torch.empty_like(di)
+    api.ml_device(di, dk, out, 1, stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    api.ml_device(di, dk, out, cfg3_iters, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    res["large_rl"] = {"workload": f"RL 512x512x128 fp32 (work box 1024x1024x256), {cfg3_iters} "
+                                   "iterations, FP32 SIMT FFT", "ms": ms,
+                       "value": img.size * cfg3_iters / (ms / 1e3) / 1e9,
+                       "unit": "Gvoxel-iter/s"}
+    return res
+
+
 def run_gpu_arm(args, rank, world):
     import torch
     from clarity_b200 import api, synthetic as syn
@@ -395,6 +445,7 @@ def run_gpu_arm(args, rank, world):
                 for k, v in fam_ms.items()}
 
     ttt = time_to_target(api, torch, img_d, psf_d, stream) if rank == 0 else None
+    others = other_configs(api, torch, stream) if rank == 0 and world == 1 else None
 
     if rank == 0:
         sample_iters = max(1, args.cpu_iters)
@@ -427,6 +478,7 @@ def run_gpu_arm(args, rank, world):
                                        f"iteration(s), {cores} host threads"},
             "clocks": clk,
             "time_to_target": ttt,
+            "other_configs": others,
         }
         print(json.dumps(line), flush=True)
     api.unregister()

@@ -56,7 +56,7 @@ EXTENSION_SYMBOLS = [
     "clarityx_jvc_device", "clarityx_idivergence", "clarityx_plan_info",
     "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
     "clarityx_convolve_noalloc", "clarityx_ml_batch_device", "clarityx_autotune",
-    "clarityx_ml_ex_device", "clarityx_ml_accel_device",
+    "clarityx_ml_ex_device", "clarityx_ml_accel_device", "clarityx_ml_u16",
     "clarityx_nn_conv3", "clarityx_nn_conv3_wgrad", "clarityx_nn_conv_in",
     "clarityx_nn_conv_in_wgrad", "clarityx_nn_head", "clarityx_nn_head_loss_grad",
     "clarityx_nn_pool2", "clarityx_nn_merge_skip_grad", "clarityx_nn_up_grad",
@@ -151,6 +151,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_ml_ex_device.restype = i
         L.clarityx_ml_accel_device.argtypes = [vp, Dim3, vp, Dim3, vp, vp, i, vp, vp]
         L.clarityx_ml_accel_device.restype = i
+        _u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
+        L.clarityx_ml_u16.argtypes = [_u16p, Dim3, _u16p, Dim3, _u16p, i]
+        L.clarityx_ml_u16.restype = i
         L.clarityx_autotune.argtypes = [i]
         L.clarityx_autotune.restype = None
         L.clarityx_launch_count.restype = C.c_longlong
@@ -435,4 +438,14 @@ def ml_accel_device(image, kernel, out, iterations, idiv=None, stream=None, star
         vp(start.data_ptr()) if start is not None else None,
         vp(out.data_ptr()), int(iterations), vp(idiv.data_ptr()) if idiv is not None else None,
         _stream_ptr(stream)))
+    return out
+
+
+def maximum_likelihood_deconvolve_u16(image, kernel, iterations: int) -> np.ndarray:
+    """clarityx_ml_u16: RL on uint16 volumes (casts on the device), as the
+    reference's DeconvolveRawImages app around Clarity_MaximumLikelihoodDeconvolve."""
+    image = np.ascontiguousarray(image, np.uint16)
+    kernel = np.ascontiguousarray(kernel, np.uint16)
+    out = np.empty_like(image)
+    _check(load().clarityx_ml_u16(image, dim3(image), kernel, dim3(kernel), out, int(iterations)))
     return out

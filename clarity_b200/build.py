@@ -91,7 +91,29 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False,
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n" + p.stdout + p.stderr)
+    if lib == LIB:
+        build_apps(lib)
     return lib
+
+
+def build_apps(lib: str = LIB) -> list[str]:
+    """The example applications (apps/*.cpp), linked against libclarity.so."""
+    out_dir = os.path.join(PKG, "bin")
+    os.makedirs(out_dir, exist_ok=True)
+    built = []
+    for src in sorted(glob.glob(os.path.join(PKG, "apps", "*.cpp"))):
+        exe = os.path.join(out_dir, os.path.splitext(os.path.basename(src))[0])
+        if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(src),
+                                                                 os.path.getmtime(lib)):
+            built.append(exe)
+            continue
+        cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+               src, "-o", exe, "-L", PKG, "-lclarity", "-Wl,-rpath,$ORIGIN/.."]
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError("app build failed:\n" + p.stdout + p.stderr)
+        built.append(exe)
+    return built
 
 
 def main() -> None:

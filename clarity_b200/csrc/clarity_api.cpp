@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <vector>
 #include <string>
@@ -406,6 +407,51 @@ ClarityResult_t clarityx_ml_device(const float* image, Clarity_Dim3 imageDim,
                          float* o) {
                        return clarity::run_rl(c, i, id, k, kd, o, iterations);
                      });
+}
+
+ClarityResult_t clarityx_ml_u16(const uint16_t* image, Clarity_Dim3 imageDim,
+                                const uint16_t* kernel, Clarity_Dim3 kernelDim, uint16_t* out,
+                                int iterations) {
+  if (!image || !kernel || !out) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (!dims_ok(imageDim) || !dims_ok(kernelDim))
+    return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  Context* ctx;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx = g_ctx;
+  }
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device());
+  ctx->clear_stream();
+  const size_t ni = (size_t)nvox(imageDim), nk = (size_t)nvox(kernelDim);
+  // uint16 data lands in the output staging buffer (sized for either
+  // volume), is cast into the image / kernel staging buffers, and the result
+  // is cast back into the image staging buffer
+  Status s = grow(&g_stage.img, &g_stage.img_cap, ni);
+  if (s.ok()) s = grow(&g_stage.ker, &g_stage.ker_cap, nk);
+  if (s.ok()) s = grow(&g_stage.out, &g_stage.out_cap, std::max(ni, nk));
+  if (!s.ok()) return report(s);
+  cudaStream_t st = ctx->exec_stream();
+  uint16_t* raw = reinterpret_cast<uint16_t*>(g_stage.out);
+  cudaError_t e = cudaMemcpyAsync(raw, image, sizeof(uint16_t) * ni, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "host to device copy"));
+  s = clarity::cast_u16_to_f32(*ctx, raw, g_stage.img, (long long)ni);
+  if (!s.ok()) return report(s);
+  e = cudaMemcpyAsync(raw, kernel, sizeof(uint16_t) * nk, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "host to device copy"));
+  s = clarity::cast_u16_to_f32(*ctx, raw, g_stage.ker, (long long)nk);
+  if (s.ok())
+    s = clarity::run_rl(*ctx, g_stage.img, to_dims(imageDim), g_stage.ker, to_dims(kernelDim),
+                        g_stage.out, iterations);
+  if (!s.ok()) return report(s);
+  uint16_t* res = reinterpret_cast<uint16_t*>(g_stage.img);
+  s = clarity::cast_f32_to_u16(*ctx, g_stage.out, res, (long long)ni);
+  if (!s.ok()) return report(s);
+  e = cudaMemcpyAsync(out, res, sizeof(uint16_t) * ni, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "device to host copy"));
+  return report(ctx->check_device_errors());
 }
 
 ClarityResult_t clarityx_ml_ex_device(const float* image, Clarity_Dim3 imageDim,

@@ -217,21 +217,6 @@ __global__ void k_reduce_sum(const float* __restrict__ a, long long n,
   block_sum_store(acc, partial);
 }
 
-__device__ __forceinline__ double block_total(const double* partial, int np) {
-  double acc = 0;
-  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partial[i];
-  __shared__ double red[32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) red[warp] = acc;
-  __syncthreads();
-  double t = 0;
-  if (threadIdx.x == 0) {
-    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) t += red[w];
-  }
-  return t;  // valid in thread 0
-}
 
 // sum -> dout[0]
 __global__ void k_finish_sum(const double* partial, int np, double* dout) {
@@ -339,6 +324,39 @@ __global__ void k_copy(const float* __restrict__ a, float* __restrict__ b,
     b[i] = a[i];
 }
 
+static constexpr int kReduceBlocks = 592;  // 4 x 148 SMs
+
+// uint16 raw volumes (the reference's DeconvolveRawImages app,
+// apps/DeconvolveRawImages/DeconvolveRawImages.cxx:91-116): cast in, and cast
+// out as x86 does for static_cast<unsigned short>(float) -- truncation to a
+// 32-bit integer (0x80000000 for NaN and |x| >= 2^31), low 16 bits kept.
+__global__ void k_u16_to_f32(const uint16_t* __restrict__ a, float* __restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+__global__ void k_f32_to_u16(const float* __restrict__ a, uint16_t* __restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float x = a[i];
+    const int v = (fabsf(x) < 2147483648.f) ? __float2int_rz(x) : INT_MIN;  // NaN fails the test
+    b[i] = (uint16_t)((unsigned)v & 0xFFFFu);
+  }
+}
+
+Status cast_u16_to_f32(Context& ctx, const uint16_t* a, float* b, long long n) {
+  count_small();
+  CLARITY_LAUNCH(k_u16_to_f32, kReduceBlocks, 256, 0, ctx.exec_stream())(a, b, n);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+Status cast_f32_to_u16(Context& ctx, const float* a, uint16_t* b, long long n) {
+  count_small();
+  CLARITY_LAUNCH(k_f32_to_u16, kReduceBlocks, 256, 0, ctx.exec_stream())(a, b, n);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
 // max of a float array: block maxima then a single-block finish.
 __global__ void k_reduce_max(const float* __restrict__ a, long long n,
                              float* __restrict__ partial) {
@@ -386,7 +404,6 @@ __global__ void k_idiv(const float* __restrict__ g, const float* __restrict__ gh
   block_sum_store(acc, partial);
 }
 
-static constexpr int kReduceBlocks = 592;  // 4 x 148 SMs
 
 // --------------------------------------------------------------- context
 Context::Context(int device) : device_(device) {
@@ -791,6 +808,8 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
   const float scale_n = inv_volume(wd);
   float* sdev = ws.fscal;  // deferred flux scale
   if (rescale) CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
+  // the last-block counter of the fused flux scale starts at zero
+  CL_CHECK(cudaMemsetAsync(ws.iscal + 2, 0, sizeof(int), st));
   CL_TRY(xy_forward(ctx, pe, ProImage{u0, P.xmode}, ws.S));
   for (int k = 0; k < iters; ++k) {
     const float* sk = (k == 0 || !rescale) ? nullptr : sdev;
@@ -822,16 +841,16 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     epi.xmode = P.xmode;
     epi.acc = 0.0;
     epi.nblocks = ws.iscal;  // the partials' count, as launched
+    if (rescale) {  // s = E / sum u' by the product pass's last block
+      epi.done = reinterpret_cast<unsigned*>(ws.iscal + 2);
+      epi.energy = ws.dscal + 0;
+      epi.sum_out = ws.dscal + 1;
+      epi.scale_out = sdev;
+    }
     if (k + 1 < iters)
       CL_TRY(xy_inv_fwd(ctx, pe, epi, ws.S));
     else
       CL_TRY(xy_inverse(ctx, pe, epi, ws.S));
-    if (rescale) {
-      count_small();
-      CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws.partial, ws.iscal, ws.dscal + 0,
-                                                       ws.dscal + 1, sdev);
-      CL_CHECK(cudaGetLastError());
-    }
   }
   if (idiv && iters > 0) {
     // idiv[iters]: the result's own I-divergence (h * s u', one more forward

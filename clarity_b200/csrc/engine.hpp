@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdint>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -139,6 +140,9 @@ Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims
 // run_rl_ex (entries k < iters at the extrapolated points).
 Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
                     const float* start, float* out, int iters, double* idiv);
+// uint16 <-> float casts of the raw-image path (x86 conversion semantics out).
+Status cast_u16_to_f32(Context& ctx, const uint16_t* a, float* b, long long n);
+Status cast_f32_to_u16(Context& ctx, const float* a, uint16_t* b, long long n);
 // Richardson-Lucy on n independent volumes of any sizes (device pointers):
 // each volume has its own plan and workspace, volumes run concurrently on the
 // batch stream pool, and with use_graph the whole batch is captured into one

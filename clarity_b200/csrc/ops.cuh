@@ -178,6 +178,26 @@ __device__ __forceinline__ void block_sum_store(double acc, double* partial) {
   }
 }
 
+// Block-wide FP64 total of np partials (thread 0 gets it; fixed order):
+// thread i sums partials i, i + blockDim.x, ..., then a tree over the block.
+// The partials are read through L2 (__ldcg): in a "last block" reduction they
+// were written by other blocks of the same kernel.
+__device__ __forceinline__ double block_total(const double* partial, int np) {
+  double acc = 0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += __ldcg(&partial[i]);
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  double t = 0;
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) t += red[w];
+  }
+  return t;  // valid in thread 0
+}
+
 // Store the real-space result on the work box.
 struct EpiWork {
   static constexpr bool has_zero_rows = false;
@@ -246,7 +266,15 @@ struct EpiRLProduct {
   WorkVol w;
   int xmode;
   double acc;
-  int* nblocks;  // receives the grid size (the number of partials), or nullptr
+  int* nblocks = nullptr;  // receives the grid size (the number of partials), or nullptr
+  // Fused flux scale (when done is not null): the last block to finish sums
+  // every block's partial in block_total's fixed order and stores
+  // *sum_out = sum, *scale_out = (float)E / (float)sum, as k_finish_rl_scale
+  // does; *done counts finished blocks and is left at 0.
+  unsigned* done = nullptr;
+  const double* energy = nullptr;
+  double* sum_out = nullptr;
+  float* scale_out = nullptr;
   __device__ __forceinline__ float cur_at(int x, int y, int z) const {
     if (cur) {
       const float u = __ldg(&cur[w.idx(x, y, z)]);
@@ -306,6 +334,24 @@ struct EpiRLProduct {
   __device__ __forceinline__ void finish() {
     block_sum_store(acc, partial);
     if (nblocks && blockIdx.x == 0 && threadIdx.x == 0) *nblocks = (int)gridDim.x;
+    if (done) {
+      // every block's reads of *scale happened before its ticket, so the last
+      // block may overwrite it
+      __shared__ int last;
+      __threadfence();  // this block's partial is visible before its ticket
+      __syncthreads();
+      if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+      __syncthreads();
+      if (last) {
+        __threadfence();
+        const double t = block_total(partial, (int)gridDim.x);
+        if (threadIdx.x == 0) {
+          *sum_out = t;
+          *scale_out = (float)*energy / (float)t;
+          *done = 0u;
+        }
+      }
+    }
   }
 };
 
@@ -352,6 +398,8 @@ struct MidRLRatio {
   // transform at all
   __device__ __forceinline__ bool zero_row(int y, int z) const { return y >= g.Y || z >= g.Z; }
   __device__ __forceinline__ bool zero_plane(int z) const { return z >= g.Z; }
+  // planes a launch needs to cover (the rest are zero_plane)
+  int live_planes(int nz) const { return g.Z < nz ? g.Z : nz; }
   // rows y0base + by*j with j < live_rows lie inside the image (y < Y)
   __device__ __forceinline__ int live_rows(int y0base, int by, int ay) const {
     const int l = (g.Y - y0base + by - 1) / by;

@@ -79,8 +79,13 @@ inline bool try_xy_tma(const PlanEntry& pe, cudaStream_t st, const F& fn, const 
     *err = allow_smem_st(k, X::SMEM);
     if (*err != cudaSuccess) return true;
     const st::Tables T = tables_of(pe);
+    // planes known to be zero need no block at all
+    int nz = SH::NZ;
+    if constexpr (requires { fn.live_planes(1); }) nz = fn.live_planes(SH::NZ);
+    const int blocks = nz * (SH::BY / X::TG);
+    if (blocks <= 0) return true;
     note_launch_begin(family, st);
-    CLARITY_LAUNCH(k, X::BLOCKS, SH::THREADS, X::SMEM, st)(fn, tm, T);
+    CLARITY_LAUNCH(k, blocks, SH::THREADS, X::SMEM, st)(fn, tm, T);
     note_launch_end(family, st);
     *err = cudaGetLastError();
     return true;

@@ -98,3 +98,20 @@ def cfg0(seed=0):
 def cfg1(seed=1):
     """256x256x64 (x,y,z), 600 spheres, 0.9 G(2,5) + 0.1 G(6,12) PSF."""
     return make_case((64, 256, 256), 600, seed=seed, halo=True)
+
+
+def cfg2_volume(i: int, seed0: int = 2000):
+    """Volume i of the batched workload: x, y uniform in 16*{6..20}, z in
+    8*{2..12}, one sphere per 8000 voxels, its own Gaussian PSF (sigma_xy in
+    [1.2, 2.5], sigma_z in [2.5, 6])."""
+    r = rng(seed0 + i)
+    x, y = 16 * int(r.integers(6, 21)), 16 * int(r.integers(6, 21))
+    z = 8 * int(r.integers(2, 13))
+    n = max(1, (x * y * z) // 8000)
+    return make_case((z, y, x), n, float(r.uniform(1.2, 2.5)), float(r.uniform(2.5, 6.0)),
+                     seed=seed0 + 10_000 + i)
+
+
+def cfg3(seed=3):
+    """512x512x128 (x,y,z), one sphere per 4000 voxels, the cfg1 halo PSF."""
+    return make_case((128, 512, 512), (512 * 512 * 128) // 4000, seed=seed, halo=True)

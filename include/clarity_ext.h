@@ -12,6 +12,8 @@
 #ifndef CLARITY_B200_CLARITY_EXT_H_
 #define CLARITY_B200_CLARITY_EXT_H_
 
+#include <stdint.h>
+
 #include "clarity.h"
 
 /* Message of the last failing call on this thread's library state, or "". */
@@ -43,6 +45,17 @@ CLARITY_API ClarityResult_t clarityx_wiener_device(
 CLARITY_API ClarityResult_t clarityx_ml_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+/* Clarity_MaximumLikelihoodDeconvolve on uint16 host volumes, as the
+ * reference's DeconvolveRawImages app does around it
+ * (apps/DeconvolveRawImages/DeconvolveRawImages.cxx:91-116), with the casts on
+ * the device: only uint16 data crosses the bus.  The result is converted as
+ * static_cast<unsigned short>(float) behaves on x86 (truncation to a 32-bit
+ * integer, low 16 bits), so the output is bit-identical to casting this
+ * library's float result on the host.  Synchronous. */
+CLARITY_API ClarityResult_t clarityx_ml_u16(const uint16_t *image, Clarity_Dim3 imageDim,
+                                            const uint16_t *kernel, Clarity_Dim3 kernelDim,
+                                            uint16_t *out, int iterations);
+
 /* Richardson-Lucy (Clarity.h.in:337-341) resumed from `start`, an estimate of
  * imageDim voxels on the device (NULL: the image, as the reference), with an
  * optional I-divergence trace: when idiv is not NULL, idiv[k] (device doubles,

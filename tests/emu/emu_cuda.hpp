@@ -77,7 +77,21 @@ inline T __ldg(const T* p) {
 inline float __shfl_xor_sync(unsigned, float, int) { return 0.f; }
 inline double __shfl_xor_sync(unsigned, double, int) { return 0.0; }
 inline void __syncthreads() {}
+// float -> int with truncation (callers keep |x| < 2^31)
+inline int __float2int_rz(float x) { return (int)x; }
+// blocks run one after another: fences order nothing further, and L2 reads
+// are plain reads
+inline void __threadfence() {}
+template <class T>
+inline T __ldcg(const T* p) {
+  return *p;
+}
 // one thread per block: atomics are plain read-modify-writes
+inline unsigned atomicAdd(unsigned* p, unsigned v) {
+  const unsigned o = *p;
+  *p = o + v;
+  return o;
+}
 inline float atomicAdd(float* p, float v) {
   const float o = *p;
   *p = o + v;

@@ -114,3 +114,11 @@ def test_planner_rejects_unsupported_prime():
     with pytest.raises(api.ClarityError) as e:
         api.plan_info((8, 8, 2 * 23))
     assert e.value.code == api.CLARITY_INVALID_ARGUMENT
+
+
+def test_raw_image_app_usage_without_gpu():
+    # the drop-in app mirrors the reference's command line (usage text, exit 1)
+    app = os.path.join(os.path.dirname(api.LIB_PATH), "bin", "deconvolve_raw_images")
+    p = subprocess.run([app], capture_output=True, text=True)
+    assert p.returncode == 1
+    assert "<image filename> <x> <y> <z> <psf filename> <x> <y> <z> <output file name>" in p.stdout

@@ -298,3 +298,33 @@ def test_accelerated_rl_vs_oracle(clarity_gpu, oracle_lib, case):
     np.testing.assert_allclose(tr.cpu().numpy(), ref_tr, rtol=1e-4)
     ref64, _ = oracle_lib.rl_accel(img, psf, iters, precision="f64")
     assert rel_l2(out.cpu().numpy(), ref64) <= 1e-3
+
+
+def _x86_u16(a):
+    """static_cast<unsigned short>(float) on x86: truncate to int32, keep the
+    low 16 bits (0x80000000 for NaN / out of range)."""
+    a = np.asarray(a, np.float32).astype(np.float64)
+    ok = np.abs(a) < 2.0 ** 31
+    v = np.where(ok, np.trunc(np.where(ok, a, 0)), -(2.0 ** 31)).astype(np.int64)
+    return (v & 0xFFFF).astype(np.uint16)
+
+
+def test_u16_raw_path_and_app(clarity_gpu, tmp_path):
+    # the raw-image path: uint16 in, device casts, uint16 out, bit-identical to
+    # casting the float path's result; and the drop-in app on raw files
+    import os
+    import subprocess
+    r = syn.rng(21)
+    img = r.integers(0, 4000, size=(12, 40, 36)).astype(np.uint16)
+    psf = (syn.gaussian_psf((12, 40, 36), 1.5, 2.0) * 60000).astype(np.uint16)
+    got = clarity_gpu.maximum_likelihood_deconvolve_u16(img, psf, 5)
+    ref = clarity_gpu.maximum_likelihood_deconvolve(img.astype(np.float32),
+                                                    psf.astype(np.float32), 5)
+    assert np.array_equal(got, _x86_u16(ref))
+    app = os.path.join(os.path.dirname(clarity_gpu.LIB_PATH), "bin", "deconvolve_raw_images")
+    img.tofile(tmp_path / "img.raw")
+    psf.tofile(tmp_path / "psf.raw")
+    p = subprocess.run([app, str(tmp_path / "img.raw"), "36", "40", "12", str(tmp_path / "psf.raw"),
+                        "36", "40", "12", str(tmp_path / "out.raw")], capture_output=True, text=True)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert np.array_equal(np.fromfile(tmp_path / "out.raw", np.uint16).reshape(img.shape), got)
