@@ -57,6 +57,7 @@ EXTENSION_SYMBOLS = [
     "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
     "clarityx_convolve_noalloc", "clarityx_ml_batch_device", "clarityx_autotune",
     "clarityx_ml_ex_device", "clarityx_ml_accel_device", "clarityx_ml_u16",
+    "clarityx_blind_ml_psf_device",
     "clarityx_nn_conv3", "clarityx_nn_conv3_wgrad", "clarityx_nn_conv_in",
     "clarityx_nn_conv_in_wgrad", "clarityx_nn_head", "clarityx_nn_head_loss_grad",
     "clarityx_nn_pool2", "clarityx_nn_merge_skip_grad", "clarityx_nn_up_grad",
@@ -154,6 +155,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         _u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
         L.clarityx_ml_u16.argtypes = [_u16p, Dim3, _u16p, Dim3, _u16p, i]
         L.clarityx_ml_u16.restype = i
+        L.clarityx_blind_ml_psf_device.argtypes = [vp, Dim3, vp, Dim3, vp, vp, i, i, vp]
+        L.clarityx_blind_ml_psf_device.restype = i
         L.clarityx_autotune.argtypes = [i]
         L.clarityx_autotune.restype = None
         L.clarityx_launch_count.restype = C.c_longlong
@@ -448,4 +451,20 @@ def maximum_likelihood_deconvolve_u16(image, kernel, iterations: int) -> np.ndar
     kernel = np.ascontiguousarray(kernel, np.uint16)
     out = np.empty_like(image)
     _check(load().clarityx_ml_u16(image, dim3(image), kernel, dim3(kernel), out, int(iterations)))
+    return out
+
+
+def blind_ml_psf_device(image, kernel, out, iterations, psf_subiterations=5, psf_out=None,
+                        stream=None):
+    """clarityx_blind_ml_psf_device: blind ML alternating one object step and
+    `psf_subiterations` PSF steps per iteration; psf_out (kernel-shaped) gets
+    the PSF estimate."""
+    for t in (image, kernel, out) + ((psf_out,) if psf_out is not None else ()):
+        if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+            raise ValueError("device variants need contiguous float32 CUDA tensors")
+    vp = C.c_void_p
+    _check(load().clarityx_blind_ml_psf_device(
+        vp(image.data_ptr()), dim3(image), vp(kernel.data_ptr()), dim3(kernel), vp(out.data_ptr()),
+        vp(psf_out.data_ptr()) if psf_out is not None else None, int(iterations),
+        int(psf_subiterations), _stream_ptr(stream)))
     return out

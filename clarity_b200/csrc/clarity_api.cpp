@@ -409,6 +409,19 @@ ClarityResult_t clarityx_ml_device(const float* image, Clarity_Dim3 imageDim,
                      });
 }
 
+ClarityResult_t clarityx_blind_ml_psf_device(const float* image, Clarity_Dim3 imageDim,
+                                             const float* kernel, Clarity_Dim3 kernelDim,
+                                             float* out, float* psf_out, int iterations,
+                                             int psf_subiterations, void* stream) {
+  if (psf_subiterations < 0) return fail(CLARITY_INVALID_ARGUMENT, "psf_subiterations < 0");
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_blind_psf(c, i, id, k, kd, o, psf_out, iterations,
+                                                     psf_subiterations);
+                     });
+}
+
 ClarityResult_t clarityx_ml_u16(const uint16_t* image, Clarity_Dim3 imageDim,
                                 const uint16_t* kernel, Clarity_Dim3 kernelDim, uint16_t* out,
                                 int iterations) {

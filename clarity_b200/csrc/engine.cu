@@ -797,23 +797,85 @@ Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
 // idiv[k] (k < iters) receives the I-divergence of the image against
 // h * (estimate at the start of iteration k), accumulated by the ratio pass,
 // and idiv[iters] that of the result.
+//
+// Blind ML's alternating updates reuse it with other roles (RLRoles): the OTF
+// may be another spectrum (the object's, for the PSF update), the start a
+// work-box volume, and the rescale target 1 (the PSF's unit sum) instead of
+// the image's energy.
+struct RLRoles {
+  const float2* otf = nullptr;  // fully transformed OTF (nullptr: ws.H)
+  Dims start_dims{0, 0, 0};     // start's extent on the work box (0: the image's)
+  bool unit_energy = false;     // rescale to sum 1 instead of sum(image)
+};
+
+__global__ void k_set_double(double* p, double v) { *p = v; }
+
+// The kernel image on the work box through the reference's pad/shift map,
+// times *scale (1 / its sum): the blind update's PSF estimate.
+__global__ void k_pad_scaled(PaddedSrc p, const float* __restrict__ scale, float* __restrict__ out) {
+  const long long n = (long long)p.nx * p.ny * p.nz;
+  const float s = *scale;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % p.nx);
+    const long long r = i / p.nx;
+    out[i] = s * p.at(x, (int)(r % p.ny), (int)(r / p.ny));
+  }
+}
+
+// out = *scale * in (work box)
+__global__ void k_scale_copy(const float* __restrict__ in, const float* __restrict__ scale,
+                             float* __restrict__ out, long long n) {
+  const float s = *scale;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = s * in[i];
+}
+
+// The PSF estimate back on the kernel's own grid: the inverse of the pad/shift
+// by -kdim/2, psf[s] = h[(s - kdim/2) mod work dim].
+__global__ void k_unpad_psf(const float* __restrict__ h, Dims wd, Dims kd, float* __restrict__ psf) {
+  const long long n = (long long)kd.x * kd.y * kd.z;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % kd.x);
+    const long long r = i / kd.x;
+    const int y = (int)(r % kd.y), z = (int)(r / kd.y);
+    const int dx = ((x - kd.x / 2) % wd.x + wd.x) % wd.x;
+    const int dy = ((y - kd.y / 2) % wd.y + wd.y) % wd.y;
+    const int dz = ((z - kd.z / 2) % wd.z + wd.z) % wd.z;
+    psf[i] = h[((long long)dz * wd.y + dy) * wd.x + dx];
+  }
+}
+
 static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
                       const float* img, Dims id, Dims wd, int iters,
-                      bool rescale, const float* start = nullptr, double* idiv = nullptr) {
+                      bool rescale, const float* start = nullptr, double* idiv = nullptr,
+                      const RLRoles& roles = RLRoles{}) {
   const VolPlan& P = pe.P;
   cudaStream_t st = ctx.exec_stream();
   const ImageSrc g = image_src(img, id);
-  const ImageSrc u0 = start ? image_src(start, id) : g;
+  const Dims sd = roles.start_dims.x > 0 ? roles.start_dims : id;
+  const ImageSrc u0 = start ? image_src(start, sd) : g;
+  const float2* H = roles.otf ? roles.otf : ws.H;
   const WorkVol wv{wd.x, wd.y, wd.z};
   const float scale_n = inv_volume(wd);
   float* sdev = ws.fscal;  // deferred flux scale
-  if (rescale) CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
+  if (rescale) {
+    if (roles.unit_energy) {
+      count_small();
+      CLARITY_LAUNCH(k_set_double, 1, 1, 0, st)(ws.dscal + 0, 1.0);
+      CL_CHECK(cudaGetLastError());
+    } else {
+      CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
+    }
+  }
   // the last-block counter of the fused flux scale starts at zero
   CL_CHECK(cudaMemsetAsync(ws.iscal + 2, 0, sizeof(int), st));
   CL_TRY(xy_forward(ctx, pe, ProImage{u0, P.xmode}, ws.S));
   for (int k = 0; k < iters; ++k) {
     const float* sk = (k == 0 || !rescale) ? nullptr : sdev;
-    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n, sk}, ws.S, ws.S));
+    CL_TRY(z_pass(ctx, pe, ModOTF{H, scale_n, sk}, ws.S, ws.S));
     MidRLRatio ratio{g, P.xmode};
     if (idiv) {
       ratio.idiv_partial = ws.partial;
@@ -828,7 +890,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     }
     // the ratio is zero in planes z >= Z (the image is zero there): P3 does
     // not write them and this pass reads them as zeros
-    ModOTF m4{ws.H, scale_n};
+    ModOTF m4{H, scale_n};
     m4.zn = id.z;
     CL_TRY(z_pass(ctx, pe, m4, ws.S, ws.S));
     EpiRLProduct epi;
@@ -856,7 +918,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     // idiv[iters]: the result's own I-divergence (h * s u', one more forward
     // transform, z pass and xy inverse that only accumulates)
     CL_TRY(xy_forward(ctx, pe, ProWork{ws.u, rescale ? sdev : nullptr, wv, P.xmode}, ws.S));
-    CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, scale_n}, ws.S, ws.S));
+    CL_TRY(z_pass(ctx, pe, ModOTF{H, scale_n}, ws.S, ws.S));
     MidRLRatio tr{g, P.xmode};
     tr.idiv_partial = ws.partial;
     tr.nblocks = ws.iscal + 1;
@@ -1203,6 +1265,81 @@ Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
 // Jansen-van Cittert: the first update reads the padded image; every update
 // is a z pass (h * i) plus one fused XY pass (inverse, JVC update, store i',
 // forward transform of i' for the next update).
+// Blind ML with the PSF update the reference leaves disabled
+// (src/BlindMaximumLikelihoodDeconvolve.cxx:50-99, the commented-out :96):
+// alternating updates -- per outer iteration one object step
+// o <- o (h * (g / (h * o))) with the current PSF, then psf_subiters PSF steps
+// h <- h (o * (g / (h * o))) renormalised to unit sum (:59) with the new
+// object.  Each step is one RL iteration of rl_core with the roles set: the
+// PSF step deconvolves by the object (its spectrum as the OTF) and rescales
+// to 1.  The object and PSF estimates live on the work box; psf_out (optional)
+// receives the PSF on the kernel's grid.
+Status run_blind_psf(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                     float* out, float* psf_out, int iters, int psf_subiters) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  cudaStream_t st = ctx.exec_stream();
+  const VolPlan& P = pe->P;
+  const long long n = wd.n();
+  if (ws->accel_cap < n) {
+    for (float*& b : ws->accel) {
+      cudaFree(b);
+      b = nullptr;
+    }
+    ws->accel_cap = 0;
+    for (float*& b : ws->accel) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
+    ws->accel_cap = n;
+  }
+  if (!ws->HG) CL_CHECK(dev_alloc((void**)&ws->HG, sizeof(float2) * (size_t)ws->spec_cap));
+  float* o = ws->accel[0];
+  float* h = ws->accel[1];
+  const WorkVol wv{wd.x, wd.y, wd.z};
+  // h = pad/shift(kernel) / sum(kernel); o = the image on the work box
+  count_small();
+  CLARITY_LAUNCH(k_reduce_sum, kReduceBlocks, 256, 0, st)(ker, kd.n(), ws->partial);
+  count_small();
+  CLARITY_LAUNCH(k_finish_inverse, 1, 256, 0, st)(ws->partial, kReduceBlocks, ws->fscal + 2);
+  count_small();
+  CLARITY_LAUNCH(k_pad_scaled, kReduceBlocks, 256, 0, st)(
+      padded(ker, kd, wd, -kd.x / 2, -kd.y / 2, -kd.z / 2), ws->fscal + 2, h);
+  count_small();
+  CLARITY_LAUNCH(k_pad_image, kReduceBlocks, 256, 0, st)(image_src(img, id), wv, o);
+  CL_CHECK(cudaGetLastError());
+  RLRoles obj;
+  obj.otf = ws->H;
+  obj.start_dims = wd;
+  RLRoles psf;
+  psf.otf = ws->HG;
+  psf.start_dims = wd;
+  psf.unit_energy = true;
+  for (int k = 0; k < iters; ++k) {
+    CL_TRY(xy_forward(ctx, *pe, ProWork{h, nullptr, wv, P.xmode}, ws->H));
+    CL_TRY(z_pass(ctx, *pe, ModForward{}, ws->H, ws->H));
+    CL_TRY(rl_core(ctx, *pe, *ws, img, id, wd, 1, false, o, nullptr, obj));
+    CL_CHECK(cudaMemcpyAsync(o, ws->u, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    if (psf_subiters > 0) {
+      CL_TRY(xy_forward(ctx, *pe, ProWork{o, nullptr, wv, P.xmode}, ws->HG));
+      CL_TRY(z_pass(ctx, *pe, ModForward{}, ws->HG, ws->HG));
+    }
+    for (int j = 0; j < psf_subiters; ++j) {
+      CL_TRY(rl_core(ctx, *pe, *ws, img, id, wd, 1, true, h, nullptr, psf));
+      count_small();
+      CLARITY_LAUNCH(k_scale_copy, kReduceBlocks, 256, 0, st)(ws->u, ws->fscal, h, n);
+      CL_CHECK(cudaGetLastError());
+    }
+  }
+  count_small();
+  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(o, wd.x, wd.y, out, id.x, id.y, id.z, nullptr);
+  if (psf_out) {
+    count_small();
+    CLARITY_LAUNCH(k_unpad_psf, kReduceBlocks, 256, 0, st)(h, wd, kd, psf_out);
+  }
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
 // Sampled Gaussian smoothing kernel of the work-box size (smoothed JVC):
 // exp(-d^2 / (2 sigma^2)) per axis about the centre n/2, a delta along an
 // axis with sigma <= 0, normalised to unit sum in double and rounded to float.

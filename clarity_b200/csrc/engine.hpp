@@ -140,6 +140,10 @@ Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims
 // run_rl_ex (entries k < iters at the extrapolated points).
 Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
                     const float* start, float* out, int iters, double* idiv);
+// Blind ML with the PSF update (alternating object and PSF steps; psf_out
+// optional, on the kernel's grid).
+Status run_blind_psf(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                     float* out, float* psf_out, int iters, int psf_subiters);
 // uint16 <-> float casts of the raw-image path (x86 conversion semantics out).
 Status cast_u16_to_f32(Context& ctx, const uint16_t* a, float* b, long long n);
 Status cast_f32_to_u16(Context& ctx, const float* a, uint16_t* b, long long n);

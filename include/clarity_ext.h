@@ -45,6 +45,17 @@ CLARITY_API ClarityResult_t clarityx_wiener_device(
 CLARITY_API ClarityResult_t clarityx_ml_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+/* Blind ML with the PSF update that Clarity_BlindMaximumLikelihoodDeconvolve
+ * leaves disabled (src/BlindMaximumLikelihoodDeconvolve.cxx:96): per outer
+ * iteration one object step o <- o (h * (g / (h * o))), then
+ * psf_subiterations PSF steps h <- h (o * (g / (h * o))) renormalised to unit
+ * sum.  psf_out (optional, kernelDim voxels) receives the PSF estimate on the
+ * kernel's grid.  No reference counterpart; device pointers, asynchronous. */
+CLARITY_API ClarityResult_t clarityx_blind_ml_psf_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, float *psf_out, int iterations,
+    int psf_subiterations, void *stream);
+
 /* Clarity_MaximumLikelihoodDeconvolve on uint16 host volumes, as the
  * reference's DeconvolveRawImages app does around it
  * (apps/DeconvolveRawImages/DeconvolveRawImages.cxx:91-116), with the casts on

@@ -276,6 +276,56 @@ void rl_accel(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
   clip<T, S>(out, id, x.data(), w.wd);
 }
 
+// Blind ML with the PSF update (no reference counterpart: the reference
+// leaves it disabled, src/BlindMaximumLikelihoodDeconvolve.cxx:96).  h starts
+// as the padded kernel over its sum (:59); per outer iteration one object step
+// o <- o (h * (g / (h * o))) (:63-93), then `sub` PSF steps
+// h <- h (o * (g / (h * o))), each renormalised to unit sum.  psf_out (kernel
+// grid) receives h through the inverse of the pad/shift.
+template <class T, class S>
+void blind_psf(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, S* psf_out, int iters,
+               int sub) {
+  Work<T> w(in, id, kernel, kd);
+  const long n = w.n;
+  std::vector<oracle::cx<T>> Hf(w.nc), Of(w.nc), tmp(w.nc);
+  std::vector<T> o(w.g), h(w.h), s1(n), s2(n);
+  {
+    const T sum = reduce_sum<T>(h.data(), n, SUM_DOUBLE);
+    const T inv = (T)1 / sum;
+    for (long i = 0; i < n; i++) h[i] = inv * h[i];
+  }
+  auto step = [&](std::vector<T>& x, const std::vector<oracle::cx<T>>& F) {
+    convolve_otf<T>(w, x.data(), F.data(), s1.data(), tmp);
+    for (long i = 0; i < n; i++)
+      s1[i] = ((double)std::fabs(s1[i]) < 1e-5) ? (T)0 : w.g[i] / s1[i];
+    convolve_otf<T>(w, s1.data(), F.data(), s2.data(), tmp);
+    for (long i = 0; i < n; i++) x[i] = x[i] * s2[i];
+  };
+  for (int k = 0; k < iters; k++) {
+    w.r2c(h.data(), Hf.data());
+    step(o, Hf);
+    if (sub > 0) w.r2c(o.data(), Of.data());
+    for (int j = 0; j < sub; j++) {
+      step(h, Of);
+      const T ne = reduce_sum<T>(h.data(), n, SUM_DOUBLE);
+      const T scale = (T)1 / ne;
+      for (long i = 0; i < n; i++) h[i] = scale * h[i];
+    }
+  }
+  clip<T, S>(out, id, o.data(), w.wd);
+  if (psf_out) {
+    for (int z = 0; z < kd.z; z++)
+      for (int y = 0; y < kd.y; y++)
+        for (int x = 0; x < kd.x; x++) {
+          const int dx = ((x - kd.x / 2) % w.wd.x + w.wd.x) % w.wd.x;
+          const int dy = ((y - kd.y / 2) % w.wd.y + w.wd.y) % w.wd.y;
+          const int dz = ((z - kd.z / 2) % w.wd.z + w.wd.z) % w.wd.z;
+          psf_out[((long)z * kd.y + y) * kd.x + x] =
+              (S)h[((long)dz * w.wd.y + dy) * w.wd.x + dx];
+        }
+  }
+}
+
 // Wiener: src/WienerDeconvolve.cxx:69-122 with the kernel of :48-66.
 template <class T, class S>
 void wiener(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, T eps,
@@ -467,6 +517,16 @@ void oracle_rl_accel_f64(const float* in, int ix, int iy, int iz, const float* k
                          int kx, int ky, int kz, float* out, int iters, double* idiv) {
   ORACLE_DIMS;
   rl_accel<double, float>(in, id, k, kd, out, iters, SUM_DOUBLE, idiv);
+}
+void oracle_blind_psf_f32(const float* in, int ix, int iy, int iz, const float* k, int kx,
+                          int ky, int kz, float* out, float* psf_out, int iters, int sub) {
+  ORACLE_DIMS;
+  blind_psf<float, float>(in, id, k, kd, out, psf_out, iters, sub);
+}
+void oracle_blind_psf_f64(const float* in, int ix, int iy, int iz, const float* k, int kx,
+                          int ky, int kz, float* out, float* psf_out, int iters, int sub) {
+  ORACLE_DIMS;
+  blind_psf<double, float>(in, id, k, kd, out, psf_out, iters, sub);
 }
 void oracle_wiener_f32(const float* in, int ix, int iy, int iz,
                        const float* k, int kx, int ky, int kz, float* out,

@@ -93,6 +93,10 @@ class Oracle:
         L.oracle_rl_accel_f64.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, i,
                                           C.c_void_p]
         L.oracle_rl_accel_f64.restype = None
+        for pr in ("f32", "f64"):
+            fn = getattr(L, f"oracle_blind_psf_{pr}")
+            fn.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, _f32p, i, i]
+            fn.restype = None
         L.oracle_idivergence.argtypes = [_f32p, _f32p, C.c_long, C.POINTER(C.c_long)]
         L.oracle_idivergence.restype = C.c_double
         L.oracle_pad_shift.argtypes = [_f32p, i, i, i, _f32p, i, i, i,
@@ -158,6 +162,17 @@ class Oracle:
             self.lib.oracle_rl_accel_f64(img, ix, iy, iz, psf, kx, ky, kz, out, int(iters),
                                          tr.ctypes.data)
         return out, tr
+
+    def blind_psf(self, img, psf, iters, sub, precision="f32"):
+        """Blind ML with the PSF update: (object estimate, PSF estimate)."""
+        img, psf = _f32(img), _f32(psf)
+        out = np.empty_like(img)
+        pout = np.empty_like(psf)
+        ix, iy, iz = _dims(img)
+        kx, ky, kz = _dims(psf)
+        getattr(self.lib, f"oracle_blind_psf_{precision}")(img, ix, iy, iz, psf, kx, ky, kz, out,
+                                                           pout, int(iters), int(sub))
+        return out, pout
 
     def wiener(self, img, psf, eps, precision="f32", work=False):
         return self._run("wiener", img, psf, [eps], precision, work)

@@ -108,6 +108,10 @@ int main(int argc, char** argv) {
   } else if (op == "accel") {  // accelerated RL, emulated device memory is host memory
     r = clarityx_ml_accel_device(img.data(), id, psf.data(), kd, nullptr, out.data(), (int)param,
                                  nullptr, nullptr);
+  } else if (op == "blindpsf") {  // blind ML with 3 PSF steps per iteration; out = object
+    std::vector<float> pout(nk);
+    r = clarityx_blind_ml_psf_device(img.data(), id, psf.data(), kd, out.data(), pout.data(),
+                                     (int)param, 3, nullptr);
   } else if (op == "batch") {
     // three volumes of different sizes in one batched call (emulated device
     // memory is host memory); each must equal its single-volume solve
