@@ -335,12 +335,15 @@ struct EpiRLProduct {
     block_sum_store(acc, partial);
     if (nblocks && blockIdx.x == 0 && threadIdx.x == 0) *nblocks = (int)gridDim.x;
     if (done) {
-      // every block's reads of *scale happened before its ticket, so the last
-      // block may overwrite it
+      // every block's reads of *scale happened before block_sum_store's
+      // barriers, so before its ticket: the last block may overwrite it.
+      // Thread 0 stored the partial; only it fences and takes the ticket, so
+      // the other threads of the block do not wait on a fence.
       __shared__ int last;
-      __threadfence();  // this block's partial is visible before its ticket
-      __syncthreads();
-      if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+      if (threadIdx.x == 0) {
+        __threadfence();  // this block's partial is visible before its ticket
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+      }
       __syncthreads();
       if (last) {
         __threadfence();

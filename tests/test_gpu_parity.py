@@ -330,8 +330,12 @@ def test_u16_raw_path_and_app(clarity_gpu, tmp_path):
     assert np.array_equal(np.fromfile(tmp_path / "out.raw", np.uint16).reshape(img.shape), got)
 
 
-@pytest.mark.parametrize("case", ["small_even", "cfg0_rl10"])
-def test_blind_ml_psf_update_vs_oracle(clarity_gpu, oracle_lib, case):
+# (case, outer iterations, PSF sub-steps).  With the PSF spanning the whole
+# volume (cfg0_rl10) the alternating updates are chaotic beyond a few steps:
+# at 3 x 5 the FP32 and FP64 oracles differ by 8x in rel-L2, so no precision
+# comparison means anything there; 3 x 2 stays conditioned (drift 9e-5).
+@pytest.mark.parametrize("case,outer,sub", [("small_even", 3, 5), ("cfg0_rl10", 3, 2)])
+def test_blind_ml_psf_update_vs_oracle(clarity_gpu, oracle_lib, case, outer, sub):
     # blind ML with the PSF update the reference leaves disabled: object and
     # PSF estimates against the oracle's restatement; the PSF keeps unit sum
     import torch
@@ -340,10 +344,10 @@ def test_blind_ml_psf_update_vs_oracle(clarity_gpu, oracle_lib, case):
     di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
     out = torch.empty_like(di)
     pout = torch.empty_like(dk)
-    clarity_gpu.blind_ml_psf_device(di, dk, out, 3, psf_subiterations=5, psf_out=pout)
+    clarity_gpu.blind_ml_psf_device(di, dk, out, outer, psf_subiterations=sub, psf_out=pout)
     torch.cuda.synchronize()
-    ref_o, ref_h = oracle_lib.blind_psf(img, psf, 3, 5)
-    o64, h64 = oracle_lib.blind_psf(img, psf, 3, 5, precision="f64")
+    ref_o, ref_h = oracle_lib.blind_psf(img, psf, outer, sub)
+    o64, h64 = oracle_lib.blind_psf(img, psf, outer, sub, precision="f64")
     # the alternating updates amplify roundoff (the FP32 oracle drifts from
     # FP64 too): held to the FP64 oracle at max(TOL_ITER, twice the FP32
     # oracle's drift)
@@ -355,6 +359,7 @@ def test_blind_ml_psf_update_vs_oracle(clarity_gpu, oracle_lib, case):
     # box may hold a little of it outside the kernel's extent
     assert 0.9 <= float(pout.sum()) <= 1.0 + 1e-4
     # without PSF steps the object update is the reference's blind ML
-    clarity_gpu.blind_ml_psf_device(di, dk, out, 3, psf_subiterations=0)
+    clarity_gpu.blind_ml_psf_device(di, dk, out, outer, psf_subiterations=0)
     torch.cuda.synchronize()
-    assert rel_l2(out.cpu().numpy(), clarity_gpu.blind_maximum_likelihood_deconvolve(img, psf, 3)) <= 1e-5
+    assert rel_l2(out.cpu().numpy(),
+                  clarity_gpu.blind_maximum_likelihood_deconvolve(img, psf, outer)) <= 1e-5
