@@ -870,8 +870,6 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
       CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
     }
   }
-  // the last-block counter of the fused flux scale starts at zero
-  CL_CHECK(cudaMemsetAsync(ws.iscal + 2, 0, sizeof(int), st));
   CL_TRY(xy_forward(ctx, pe, ProImage{u0, P.xmode}, ws.S));
   for (int k = 0; k < iters; ++k) {
     const float* sk = (k == 0 || !rescale) ? nullptr : sdev;
@@ -903,16 +901,19 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     epi.xmode = P.xmode;
     epi.acc = 0.0;
     epi.nblocks = ws.iscal;  // the partials' count, as launched
-    if (rescale) {  // s = E / sum u' by the product pass's last block
-      epi.done = reinterpret_cast<unsigned*>(ws.iscal + 2);
-      epi.energy = ws.dscal + 0;
-      epi.sum_out = ws.dscal + 1;
-      epi.scale_out = sdev;
-    }
     if (k + 1 < iters)
       CL_TRY(xy_inv_fwd(ctx, pe, epi, ws.S));
     else
       CL_TRY(xy_inverse(ctx, pe, epi, ws.S));
+    if (rescale) {
+      // s = E / sum u' by one block in a fixed order.  A last-block ticket
+      // in the product pass itself cost more: each of its blocks then waited
+      // for an atomic's round trip before it could exit.
+      count_small();
+      CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws.partial, ws.iscal, ws.dscal + 0,
+                                                       ws.dscal + 1, sdev);
+      CL_CHECK(cudaGetLastError());
+    }
   }
   if (idiv && iters > 0) {
     // idiv[iters]: the result's own I-divergence (h * s u', one more forward

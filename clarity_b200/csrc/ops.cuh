@@ -180,8 +180,8 @@ __device__ __forceinline__ void block_sum_store(double acc, double* partial) {
 
 // Block-wide FP64 total of np partials (thread 0 gets it; fixed order):
 // thread i sums partials i, i + blockDim.x, ..., then a tree over the block.
-// The partials are read through L2 (__ldcg): in a "last block" reduction they
-// were written by other blocks of the same kernel.
+// The partials are read through L2 (__ldcg); they come from the previous
+// kernel on the stream.
 __device__ __forceinline__ double block_total(const double* partial, int np) {
   double acc = 0;
   for (int i = threadIdx.x; i < np; i += blockDim.x) acc += __ldcg(&partial[i]);
@@ -267,14 +267,6 @@ struct EpiRLProduct {
   int xmode;
   double acc;
   int* nblocks = nullptr;  // receives the grid size (the number of partials), or nullptr
-  // Fused flux scale (when done is not null): the last block to finish sums
-  // every block's partial in block_total's fixed order and stores
-  // *sum_out = sum, *scale_out = (float)E / (float)sum, as k_finish_rl_scale
-  // does; *done counts finished blocks and is left at 0.
-  unsigned* done = nullptr;
-  const double* energy = nullptr;
-  double* sum_out = nullptr;
-  float* scale_out = nullptr;
   __device__ __forceinline__ float cur_at(int x, int y, int z) const {
     if (cur) {
       const float u = __ldg(&cur[w.idx(x, y, z)]);
@@ -334,27 +326,6 @@ struct EpiRLProduct {
   __device__ __forceinline__ void finish() {
     block_sum_store(acc, partial);
     if (nblocks && blockIdx.x == 0 && threadIdx.x == 0) *nblocks = (int)gridDim.x;
-    if (done) {
-      // every block's reads of *scale happened before block_sum_store's
-      // barriers, so before its ticket: the last block may overwrite it.
-      // Thread 0 stored the partial; only it fences and takes the ticket, so
-      // the other threads of the block do not wait on a fence.
-      __shared__ int last;
-      if (threadIdx.x == 0) {
-        __threadfence();  // this block's partial is visible before its ticket
-        last = atomicAdd(done, 1u) == gridDim.x - 1;
-      }
-      __syncthreads();
-      if (last) {
-        __threadfence();
-        const double t = block_total(partial, (int)gridDim.x);
-        if (threadIdx.x == 0) {
-          *sum_out = t;
-          *scale_out = (float)*energy / (float)t;
-          *done = 0u;
-        }
-      }
-    }
   }
 };
 

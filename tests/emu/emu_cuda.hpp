@@ -31,23 +31,31 @@ struct Launcher {
     const dim3 g = grid;
     const size_t s = smem;
     return [g, s, kernel](auto... args) {
-      for (unsigned bz = 0; bz < g.z; ++bz)
-        for (unsigned by = 0; by < g.y; ++by)
-          for (unsigned bx = 0; bx < g.x; ++bx) {
-            bIdx = make_uint3(bx, by, bz);
-            tIdx = make_uint3(0, 0, 0);
-            bDim = dim3(1, 1, 1);
-            gDim = g;
-            void* p = nullptr;
-            if (s) {
-              p = std::aligned_alloc(128, (s + 127) / 128 * 128);  // as __align__(128)
-              std::memset(p, 0xff, s);
-            }
-            smem_ptr = p;
-            kernel(args...);
-            std::free(p);
-            smem_ptr = nullptr;
-          }
+      // EMU_BLOCK_ORDER=reverse runs the blocks last to first: a kernel whose
+      // result depends on the order of its blocks has an inter-block race
+      static const bool reverse = [] {
+        const char* v = std::getenv("EMU_BLOCK_ORDER");
+        return v && v[0] == 'r';
+      }();
+      const unsigned long long nb = (unsigned long long)g.x * g.y * g.z;
+      for (unsigned long long q = 0; q < nb; ++q) {
+        const unsigned long long b = reverse ? nb - 1 - q : q;
+        const unsigned bx = (unsigned)(b % g.x), by = (unsigned)((b / g.x) % g.y),
+                       bz = (unsigned)(b / ((unsigned long long)g.x * g.y));
+        bIdx = make_uint3(bx, by, bz);
+        tIdx = make_uint3(0, 0, 0);
+        bDim = dim3(1, 1, 1);
+        gDim = g;
+        void* p = nullptr;
+        if (s) {
+          p = std::aligned_alloc(128, (s + 127) / 128 * 128);  // as __align__(128)
+          std::memset(p, 0xff, s);
+        }
+        smem_ptr = p;
+        kernel(args...);
+        std::free(p);
+        smem_ptr = nullptr;
+      }
     };
   }
 };

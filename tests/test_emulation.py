@@ -144,3 +144,20 @@ def test_emulated_nn_conv3_matches_reference(emu, tmp_path, dims, chans):
     dw = rd("dw", (co, 27, cin))
     assert (dw - w.grad).abs().max() <= 1e-4 * w.grad.abs().max()
     assert (rd("db", (co,)) - dy.sum(dim=(0, 1, 2))).abs().max() <= 1e-4 * dy.abs().sum()
+
+
+@pytest.mark.parametrize("shape", [(12, 20, 24), (8, 30, 30)])
+def test_emulated_results_do_not_depend_on_block_order(emu, tmp_path, shape):
+    # every block of a pass owns its slice of the spectrum and of the output:
+    # running the blocks last to first must give the same bits
+    r = syn.rng(21)
+    img = r.integers(0, 4000, size=shape).astype(np.float32)
+    psf = syn.gaussian_psf(shape, 1.5, 2.0).astype(np.float32)
+    for op, prm in (("convolve", 0), ("rl", 2), ("jvc", 2)):
+        fwd = run_emu(emu, tmp_path, op, img, psf, prm)
+        os.environ["EMU_BLOCK_ORDER"] = "reverse"
+        try:
+            rev = run_emu(emu, tmp_path, op, img, psf, prm)
+        finally:
+            del os.environ["EMU_BLOCK_ORDER"]
+        assert np.array_equal(fwd, rev), op

@@ -327,7 +327,14 @@ def test_u16_raw_path_and_app(clarity_gpu, tmp_path):
     p = subprocess.run([app, str(tmp_path / "img.raw"), "36", "40", "12", str(tmp_path / "psf.raw"),
                         "36", "40", "12", str(tmp_path / "out.raw")], capture_output=True, text=True)
     assert p.returncode == 0, p.stdout + p.stderr
-    assert np.array_equal(np.fromfile(tmp_path / "out.raw", np.uint16).reshape(img.shape), got)
+    app = np.fromfile(tmp_path / "out.raw", np.uint16).reshape(img.shape)
+    # another process may round the float result differently in the last
+    # bits (within the float path's tolerance); truncation then moves a value
+    # by one only where that result lies next to an integer
+    diff = app.astype(np.int64) - got.astype(np.int64)
+    assert np.abs(diff).max() <= 1
+    near = np.abs(ref - np.round(ref)) <= 1e-5 * np.maximum(1.0, np.abs(ref))
+    assert np.all(near[diff != 0])
 
 
 # (case, outer iterations, PSF sub-steps).  With the PSF spanning the whole
