@@ -283,10 +283,14 @@ __global__ void k_finish_sum_np(const double* partial, const int* np, double* do
 
 // RL flux scale (src/MaximumLikelihoodDeconvolve.cxx:73-78):
 // scale = energy / newEnergy with both rounded to float first, as the
-// reference holds them in floats.
-__global__ void k_finish_rl_scale(const double* partial, const int* np,
-                                  const double* energy, double* sum_out,
-                                  float* scale_out) {
+// reference holds them in floats.  It runs once per RL iteration on the
+// critical path between two passes, so a full 1024-thread block reads the
+// partials (4096 at the 512x512x128 box: four per thread); block_total
+// handles up to 32 warps.
+static constexpr int kFinishThreads = 1024;
+__global__ void __launch_bounds__(kFinishThreads)
+    k_finish_rl_scale(const double* partial, const int* np, const double* energy,
+                      double* sum_out, float* scale_out) {
   const double t = block_total(partial, *np);
   if (threadIdx.x == 0) {
     sum_out[0] = t;
@@ -910,8 +914,8 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
       // in the product pass itself cost more: each of its blocks then waited
       // for an atomic's round trip before it could exit.
       count_small();
-      CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws.partial, ws.iscal, ws.dscal + 0,
-                                                       ws.dscal + 1, sdev);
+      CLARITY_LAUNCH(k_finish_rl_scale, 1, kFinishThreads, 0, st)(
+          ws.partial, ws.iscal, ws.dscal + 0, ws.dscal + 1, sdev);
       CL_CHECK(cudaGetLastError());
     }
   }
@@ -1075,8 +1079,8 @@ Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, D
     epi.nblocks = ws->iscal;
     CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
     count_small();
-    CLARITY_LAUNCH(k_finish_rl_scale, 1, 256, 0, st)(ws->partial, ws->iscal, ws->dscal + 0,
-                                                     ws->dscal + 1, sdev);
+    CLARITY_LAUNCH(k_finish_rl_scale, 1, kFinishThreads, 0, st)(
+        ws->partial, ws->iscal, ws->dscal + 0, ws->dscal + 1, sdev);
     count_small();
     CLARITY_LAUNCH(k_accel_update, kReduceBlocks, 256, 0, st)(B[ui], Y, G, sdev, k == 0 ? 1 : 0,
                                                               n, ws->partial);
