@@ -877,7 +877,11 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
   CL_TRY(xy_forward(ctx, pe, ProImage{u0, P.xmode}, ws.S));
   for (int k = 0; k < iters; ++k) {
     const float* sk = (k == 0 || !rescale) ? nullptr : sdev;
-    CL_TRY(z_pass(ctx, pe, ModOTF{H, scale_n, sk}, ws.S, ws.S));
+    // P3 reads only planes z < Z (the image is zero beyond): the rest of this
+    // pass's output is neither inverse-transformed along y0 nor stored
+    ModOTF m2{H, scale_n, sk};
+    m2.zout = id.z;
+    CL_TRY(z_pass(ctx, pe, m2, ws.S, ws.S));
     MidRLRatio ratio{g, P.xmode};
     if (idiv) {
       ratio.idiv_partial = ws.partial;
@@ -1052,7 +1056,9 @@ Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, D
   CL_CHECK(cudaMemsetAsync(alpha, 0, sizeof(float), st));
   for (int k = 0; k < iters; ++k) {
     CL_TRY(xy_forward(ctx, *pe, ProAccel{B[xi], B[pi], alpha, Y, wv, P.xmode}, ws->S));
-    CL_TRY(z_pass(ctx, *pe, ModOTF{ws->H, scale_n}, ws->S, ws->S));
+    ModOTF m2{ws->H, scale_n};
+    m2.zout = id.z;  // the ratio pass reads planes z < Z only
+    CL_TRY(z_pass(ctx, *pe, m2, ws->S, ws->S));
     MidRLRatio ratio{g, P.xmode};
     if (idiv) {
       ratio.idiv_partial = ws->partial;

@@ -478,6 +478,9 @@ struct ModOTF {
   // only the first zn z planes of the input spectrum are nonzero (the rest
   // were never written and are read as zeros)
   int zn = 1 << 30;
+  // only the first zout z planes of the output are read by the next pass:
+  // the rest are neither inverse-transformed along y0 nor stored
+  int zout = 1 << 30;
   // the OTF tile this block will multiply by, into L2 (part p of np)
   __device__ __forceinline__ void prefetch_tile(unsigned base, int tile, int p, int np) const {
     const size_t chunk = ((size_t)tile * 8 / np + 15) & ~size_t(15);
@@ -513,6 +516,7 @@ struct ModWiener {
   const float2* __restrict__ H;
   float eps, scale;
   int zn = 1 << 30;
+  int zout = 1 << 30;
   __device__ __forceinline__ void prefetch_tile(unsigned base, int tile, int p, int np) const {
     const size_t chunk = ((size_t)tile * 8 / np + 15) & ~size_t(15);
     const size_t off = chunk * p, total = (size_t)tile * 8;
@@ -533,6 +537,7 @@ struct ModWiener {
 struct ModForward {
   static constexpr bool forward_only = true;
   int zn = 1 << 30;
+  int zout = 1 << 30;
   __device__ __forceinline__ void prefetch_tile(unsigned, int, int, int) const {}
   __device__ __forceinline__ float2 apply(long long, float2 v) const { return v; }
   __device__ __forceinline__ ModForward resolved() const { return *this; }

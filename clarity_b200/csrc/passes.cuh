@@ -584,13 +584,15 @@ __global__ void __launch_bounds__(256, 2)
     smem_inverse<false>(sm, P, P.az, 0, BW, BW, 1, 0, BW, true, twz);
     smem_inverse<false>(sm, P, P.ayB, 0, P.nz * P.W, P.W, 1, BW, P.W, true, twy);
   }
-  if ((tile & 1) == 0) {
+  // planes z >= zout are not needed downstream: not stored
+  const long long out = (long long)(mod.zout < P.nz ? mod.zout : P.nz) * P.By * P.W;
+  if ((tile & 1) == 0 && (out & 1) == 0) {
     float4* dst = reinterpret_cast<float4*>(Sout + base);
     const float4* src = reinterpret_cast<const float4*>(sm);
-    const int n4 = (int)(tile / 2);
+    const int n4 = (int)(out / 2);
     for (int t = threadIdx.x; t < n4; t += blockDim.x) dst[t] = src[t];
   } else {
-    for (int t = threadIdx.x; t < tile; t += blockDim.x) Sout[base + t] = sm[t];
+    for (int t = threadIdx.x; t < out; t += blockDim.x) Sout[base + t] = sm[t];
   }
 }
 

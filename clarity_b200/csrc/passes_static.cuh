@@ -659,10 +659,13 @@ __global__ void __launch_bounds__(256, 2)
     tile_inverse_down_to<SH, typename SH::Y, 0, false>(sm, T.twy);
   }
   {
+    // planes z >= zout are not needed downstream (BW even: whole float4s)
+    const int zo = mod.zout < SH::NZ ? mod.zout : SH::NZ;
+    const int out4 = zo * SH::BW / 2;
     float4* dst = reinterpret_cast<float4*>(Sout + base);
     const float4* src = reinterpret_cast<const float4*>(sm);
 #pragma unroll 4
-    for (int t = threadIdx.x; t < tile / 2; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) dst[t] = src[t];
+    for (int t = threadIdx.x; t < out4; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) dst[t] = src[t];
   }
 }
 
@@ -823,9 +826,10 @@ __global__ void __launch_bounds__(256, 2)
       z2_pass<SH, 0, +1>(sm, twz);
       __syncthreads();
     }
-    // y0 inverse per line
+    // y0 inverse per line, for the planes the next pass reads (z < zo)
+    const int zo = mod.zout < NZ ? mod.zout : NZ;
 #pragma unroll 1
-    for (int l = threadIdx.x; l < NZ * W; l += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    for (int l = threadIdx.x; l < zo * W; l += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
       const int ki = l % W, z = l / W;
       float2* d = sm + z * ZS + ki;
       float2 v[BY];
@@ -845,7 +849,7 @@ __global__ void __launch_bounds__(256, 2)
       fence_smem_to_async();
       __syncthreads();
       if ((int)threadIdx.x < CLARITY_ISSUE_LANES) {
-        for (int z = threadIdx.x; z < NZ; z += CLARITY_ISSUE_LANES)
+        for (int z = threadIdx.x; z < zo; z += CLARITY_ISSUE_LANES)
           bulk_store(Sout + gbase + z * BW, sm + z * ZS, BW * 8);
         bulk_store_commit_and_wait();
       }
