@@ -87,16 +87,23 @@ __device__ __forceinline__ void per_task_two_phase(const A& a, const B& b) {
 #endif
 }
 
-// Runs f(row, k, pa, pb, w) for every tile row and pair 0 < k < M/2 of slots
-// pa = slot(k), pb = slot(M - k), w = twr[k].  With KP (the power of two >= the
+// Runs f(row, k, pa, pb, w) for the tile rows j < L of every line and every
+// pair 0 < k < M/2 of slots pa = slot(k), pb = slot(M - k), w = twr[k] (rows
+// j >= L are known zeros or not needed).  With KP (the power of two >= the
 // pair count) dividing the block, each thread keeps one k for all its rows,
 // so the slots and the twiddle are computed once.
 template <class SH, class F>
 __device__ __forceinline__ void for_each_pair(float2* buf, const float2* __restrict__ twr,
-                                              const F& f) {
+                                              const F& f, int L = XyTma<SH>::AY) {
   using X = XyTma<SH>;
   using T = typename X::T;
-  constexpr int M = X::M, NP = M / 2 - 1, NR = X::NROWS;
+  constexpr int M = X::M, NP = M / 2 - 1, AY = X::AY;
+  const int NR = X::TG * L;  // rows visited
+  // visited row rv -> tile row g * AY + j, j < L
+  auto row_of = [&](int rv) {
+    const int g = rv / L;
+    return g * AY + (rv - g * L);
+  };
   constexpr int KP = NP < 2 ? 1 : (1 << (32 - __builtin_clz(NP - 1)));
   constexpr int TH = SH::THREADS;
 #ifndef CLARITY_HOST_EMULATION
@@ -111,24 +118,27 @@ __device__ __forceinline__ void for_each_pair(float2* buf, const float2* __restr
       const int pa = xp<T>(xrev<T>(k)), pb = xp<T>(xrev<T>(M - k));
       const float2 w = __ldg(&twr[k]);
 #pragma unroll 2
-      for (int r = (int)threadIdx.x / KP; r < NR; r += RSTEP) f(buf + row_off<T>(r), pa, pb, w);
+      for (int rv = (int)threadIdx.x / KP; rv < NR; rv += RSTEP)
+        f(buf + row_off<T>(row_of(rv)), pa, pb, w);
     }
   } else {
 #pragma unroll 1
     for (int q = threadIdx.x; q < NR * NP; q += CLARITY_BLOCK_STRIDE(TH)) {
       const int k = 1 + q % NP;
-      const int r = q / NP;
+      const int r = row_of(q / NP);
       f(buf + row_off<T>(r), xp<T>(xrev<T>(k)), xp<T>(xrev<T>(M - k)), __ldg(&twr[k]));
     }
   }
 }
 
 // Inverse column step: box (natural kx) -> x rows (digit-reversed slots),
-// then the c2r pair combine of slots k and M - k.
+// then the c2r pair combine of slots k and M - k.  Only rows j < L of each
+// line are written (the later steps read no others).
 template <class SH>
 __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
                                                  const float2* __restrict__ twr,
-                                                 const float2* __restrict__ twny) {
+                                                 const float2* __restrict__ twny,
+                                                 int L = XyTma<SH>::AY) {
   using X = XyTma<SH>;
   using T = typename X::T;
   constexpr int M = X::M, AY = X::AY, RS = T::ROWSTRIDE;
@@ -160,15 +170,18 @@ __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
     if (cc == 0) {
       const int p0 = xp<T>(0);
 #pragma unroll
-      for (int j = 0; j < AY; ++j) rows[j * RS + p0] = make_float2(v[j].x + v[j].y, v[j].x - v[j].y);
+      for (int j = 0; j < AY; ++j)
+        if (j < L) rows[j * RS + p0] = make_float2(v[j].x + v[j].y, v[j].x - v[j].y);
     } else if (cc == 1) {
       const int ph = xp<T>(xrev<T>(M / 2));
 #pragma unroll
-      for (int j = 0; j < AY; ++j) rows[j * RS + ph] = make_float2(2.f * v[j].x, -2.f * v[j].y);
+      for (int j = 0; j < AY; ++j)
+        if (j < L) rows[j * RS + ph] = make_float2(2.f * v[j].x, -2.f * v[j].y);
     } else {
       const int p = xp<T>(xrev<T>(task_kx(cc, M)));
 #pragma unroll
-      for (int j = 0; j < AY; ++j) rows[j * RS + p] = v[j];
+      for (int j = 0; j < AY; ++j)
+        if (j < L) rows[j * RS + p] = v[j];
     }
   };
   per_task_two_phase<X::TASKS, AY>(load, store);
@@ -180,16 +193,18 @@ __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
     const float2 o = cmulc(csub(xa, b), w);
     row[pa] = make_float2(e.x - o.y, e.y + o.x);
     row[pb] = make_float2(e.x + o.y, -e.y + o.x);
-  });
+  }, L);
   __syncthreads();
 }
 
 // Forward column step: x rows (digit-reversed slots) -> box (natural kx),
-// every kx < KG*W written (slots beyond M are zero).
+// every kx < KG*W written (slots beyond M are zero).  Rows j >= L of each
+// line hold zeros: the pair split leaves them so and skips them.
 template <class SH>
 __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
                                                  const float2* __restrict__ twr,
-                                                 const float2* __restrict__ twny) {
+                                                 const float2* __restrict__ twny,
+                                                 int L = XyTma<SH>::AY) {
   using X = XyTma<SH>;
   using T = typename X::T;
   constexpr int M = X::M, AY = X::AY, RS = T::ROWSTRIDE;
@@ -203,7 +218,7 @@ __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
     const float2 wo = cmul(w, o);
     row[pa] = cadd(e, wo);
     row[pb] = conjf2(csub(e, wo));
-  });
+  }, L);
   __syncthreads();
   auto load = [&](int c, float2* v) {
     const int g = c / M, cc = c - g * M;
@@ -397,11 +412,12 @@ __global__ void __launch_bounds__(256, 3)
     mbar_wait(&bars[1], 0, nullptr);
     return;
   }
-  cols_inverse_tma<SH>(buf, y0base, T.twr, T.twny);
-  const RowSkip<TS, Epi> skip{epi, z, y0base};
+  // rows j >= L of every line are outside the image (zero for this epilogue)
   int L = SH::AY;
   if constexpr (Epi::has_zero_rows) L = epi.live_rows(y0base, SH::BY, SH::AY);
   constexpr bool CP = Epi::has_zero_rows;
+  cols_inverse_tma<SH>(buf, y0base, T.twr, T.twny, L);
+  const RowSkip<TS, Epi> skip{epi, z, y0base};
   x_inverse_down_to<TS, 1, RowSkip<TS, Epi>, CP>(buf, T.twx, skip, L);
   if (!mbar_wait(&bars[1], 0, T.err)) {
     mbar_wait(&bars[1], 0, nullptr);
@@ -439,7 +455,7 @@ __global__ void __launch_bounds__(256, 3)
     }
     __syncthreads();
     x_forward_from<TS, 1, RowSkip<TS, Epi>, CP>(buf, T.twx, skip, L);
-    cols_forward_tma<SH>(buf, y0base, T.twr, T.twny);
+    cols_forward_tma<SH>(buf, y0base, T.twr, T.twny, L);
     fence_smem_to_async();
     __syncthreads();
     if (threadIdx.x == 0) {

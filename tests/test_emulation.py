@@ -161,3 +161,17 @@ def test_emulated_results_do_not_depend_on_block_order(emu, tmp_path, shape):
         finally:
             del os.environ["EMU_BLOCK_ORDER"]
         assert np.array_equal(fwd, rev), op
+
+
+@pytest.mark.parametrize("ishape,kshape", [((20, 30, 40), (12, 34, 24)),
+                                           ((17, 29, 41), (15, 35, 23))])
+def test_emulated_specialised_box_with_uneven_split(emu, tmp_path, ishape, kshape, oracle_lib):
+    # a 64x64x32 work box (a specialised shape: TMA XY pass, per-line Z pass)
+    # reached from image and PSF extents that are not multiples of the tile:
+    # the ratio pass's live rows differ between lines and row groups
+    r = syn.rng(5)
+    img = (r.random(ishape) * 100).astype(np.float32)
+    psf = syn.gaussian_psf(kshape, 1.5, 2.0).astype(np.float32)
+    assert rel_l2(run_emu(emu, tmp_path, "rl", img, psf, 3), oracle_lib.rl(img, psf, 3)) <= 2e-6
+    out, _ = oracle_lib.rl_accel(img, psf, 2)
+    assert rel_l2(run_emu(emu, tmp_path, "accel", img, psf, 2), out) <= 2e-6
