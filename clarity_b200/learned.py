@@ -7,8 +7,8 @@ iterate 5 (the network's input) and iterate 200 (its target) with batched RL
 on the GPU.  The network (unet.UNet3D) learns the per-voxel log-ratio between
 the two.  At solve time RL runs `pre` iterations, the network predicts an
 advanced estimate, and RL resumes from it (clarityx_ml_ex_device with a start
-estimate); plain RL remains the fallback and the judge (the I-divergence
-trace of both).
+estimate); plain RL remains the fallback, and the I-divergence traces of
+both tell which is ahead.
 
     python -m clarity_b200.learned --patches 2000 --epochs 6 --out weights.npy
 """

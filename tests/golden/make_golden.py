@@ -60,7 +60,7 @@ def main():
     k = syn.gaussian_psf((8, 8, 8), 2.0, 2.0).astype(np.float32)
     conv = O.ReferenceCPU("ref").convolve(t, k)
     case("testcommon_16x16x8", conv, k, 10, 10, 10)
-    # 64x64x32, 40 spheres, sigma 1.5/3.0, RL 10 iterations
+    # the small RL workload: 64x64x32, 40 spheres, sigma 1.5/3.0, RL 10 iterations
     img, psf, _ = syn.cfg0(seed=0)
     case("cfg0_rl10", img, psf, 10, 10, 10, full=False)
 

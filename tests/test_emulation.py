@@ -74,7 +74,7 @@ def test_emulated_library_matches_reference_golden(emu, tmp_path, case):
 
 @pytest.mark.parametrize("img_zyx,psf_zyx", [
     ((16, 32, 32), (16, 32, 32)),   # work 64x64x32: compile-time specialised shape
-    ((32, 64, 64), (32, 64, 64)),   # work 128x128x64: specialised shape of configs[0]
+    ((32, 64, 64), (32, 64, 64)),   # work 128x128x64: specialised shape of the small RL workload
     ((12, 24, 20), (12, 24, 20)),   # work 40x48x24: Ay 12, x radix 5*4
     ((10, 30, 18), (10, 30, 18)),   # work 36x60x20: Ay 4, By 15 (2 passes)
     ((15, 27, 25), (15, 27, 25)),   # work 50x54x30: Ay 3, By 18

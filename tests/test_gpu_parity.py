@@ -66,7 +66,7 @@ def test_blind_golden(clarity_gpu, case):
 
 
 def test_cfg0_rl10_golden(clarity_gpu, oracle_lib):
-    # 64x64x32 image, same-size PSF, 10 RL iterations
+    # the small RL workload: 64x64x32 image, same-size PSF, 10 RL iterations
     d = load_golden("cfg0_rl10")
     out = clarity_gpu.maximum_likelihood_deconvolve(d["image"], d["psf"], 10)
     err32 = rel_l2(out, d["rl_ref64"])
@@ -96,7 +96,7 @@ def test_odd_shapes_vs_oracle(clarity_gpu, oracle_lib, img_shape, psf_shape):
 
 
 def test_cfg1_rl_one_iteration_vs_oracle(clarity_gpu, oracle_lib):
-    # configs[1] size (256x256x64 image, same-size halo PSF): one iteration
+    # the benchmark size (256x256x64 image, same-size halo PSF): one iteration
     # against the FP32 restatement (double flux sum)
     img, psf, _ = syn.cfg1(seed=1)
     out = clarity_gpu.maximum_likelihood_deconvolve(img, psf, 1)
@@ -105,7 +105,7 @@ def test_cfg1_rl_one_iteration_vs_oracle(clarity_gpu, oracle_lib):
 
 
 def test_cfg1_rl_three_iterations_vs_oracle(clarity_gpu, oracle_lib):
-    # configs[1] size: the steady-iteration kernels (ratio pass, product pass
+    # the benchmark size: the steady-iteration kernels (ratio pass, product pass
     # reading the previous estimate and the deferred flux scale) at full size
     img, psf, _ = syn.cfg1(seed=3)
     out = clarity_gpu.maximum_likelihood_deconvolve(img, psf, 3)
@@ -187,7 +187,7 @@ def _batch_inputs(seed, shapes):
 
 
 def test_batched_rl_uneven_volumes(clarity_gpu, oracle_lib):
-    # configs[2] form at small sizes: volumes of uneven sizes in one call, run
+    # the batched workload at small sizes: volumes of uneven sizes in one call, run
     # directly and as a captured CUDA graph (captured, then replayed)
     import torch
     shapes = [(8, 24, 16), (12, 20, 28), (16, 32, 32), (6, 18, 22), (10, 16, 24)]
