@@ -136,8 +136,9 @@ __device__ __forceinline__ int visit_row(int rv, int L) {
   return g * SH::AY + (rv - g * L);
 }
 
+// tw: the x twiddle table w_M^t, in global or shared memory (plain loads).
 template <class SH, int S, int DIR, class Skip, bool COMPACT = false>
-__device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw,
+__device__ __forceinline__ void x_pass(float2* sm, const float2* tw,
                                        const Skip& skip, int L = SH::AY) {
   using X = typename SH::X;
   constexpr int R = X::radix(S), len = X::len(S), span = len / R;
@@ -160,12 +161,12 @@ __device__ __forceinline__ void x_pass(float2* sm, const float2* __restrict__ tw
       dft<R, -1>(v);
       if (span > 1 && i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k * twstep]));
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], tw[i * k * twstep]);
       }
     } else {
       if (span > 1 && i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k * twstep]));
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], tw[i * k * twstep]);
       }
       dft<R, +1>(v);
     }

@@ -46,6 +46,10 @@ struct XyTma {
   static constexpr int STG_F = NROWS * NX;
   static constexpr int SMEM = BUF_F2 * 8 + STG_F * 4;
   static constexpr int TASKS = TG * M;  // column DFTs per tile
+  // x twiddles (M) and the lines' y split twiddles (TG*AY) staged in shared
+  // memory when three blocks per SM still fit beside the dynamic tile
+  static constexpr int TW_F2 = M + TG * AY;
+  static constexpr bool TW_SMEM = 3 * (SMEM + TW_F2 * 8 + 2048 + 1024) <= 228 * 1024;
   static constexpr int THREADS = SH::THREADS;
   static constexpr int BLOCKS = SH::NZ * (SH::BY / TG);
   // usable when the tile fits three blocks per SM, every column task has a
@@ -137,7 +141,7 @@ __device__ __forceinline__ void for_each_pair(float2* buf, const float2* __restr
 template <class SH>
 __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
                                                  const float2* __restrict__ twr,
-                                                 const float2* __restrict__ twny,
+                                                 const float2* twl,
                                                  int L = XyTma<SH>::AY) {
   using X = XyTma<SH>;
   using T = typename X::T;
@@ -149,7 +153,7 @@ __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
 #pragma unroll
     for (int k1 = 0; k1 < AY; ++k1) {
       float2 a = buf[X::box(k1, kx, g)];
-      if (k1 != 0 && y0 != 0) a = cmulc(a, __ldg(&twny[y0 * k1]));
+      if (k1 != 0 && y0 != 0) a = cmulc(a, twl[g * AY + k1]);
       v[k1] = a;
     }
     if (cc == 0) {
@@ -157,7 +161,7 @@ __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
 #pragma unroll
       for (int k1 = 0; k1 < AY; ++k1) {
         float2 b = buf[X::box(k1, M, g)];
-        if (k1 != 0 && y0 != 0) b = cmulc(b, __ldg(&twny[y0 * k1]));
+        if (k1 != 0 && y0 != 0) b = cmulc(b, twl[g * AY + k1]);
         v[k1] = make_float2(v[k1].x - b.y, v[k1].y + b.x);
       }
     }
@@ -203,7 +207,7 @@ __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
 template <class SH>
 __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
                                                  const float2* __restrict__ twr,
-                                                 const float2* __restrict__ twny,
+                                                 const float2* twl,
                                                  int L = XyTma<SH>::AY) {
   using X = XyTma<SH>;
   using T = typename X::T;
@@ -261,7 +265,7 @@ __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
     const int kx = cc == 0 ? 0 : (cc == 1 ? M / 2 : task_kx(cc, M));
 #pragma unroll
     for (int k1 = 0; k1 < AY; ++k1) {
-      const float2 w = (k1 == 0 || y0 == 0) ? make_float2(1.f, 0.f) : __ldg(&twny[y0 * k1]);
+      const float2 w = (k1 == 0 || y0 == 0) ? make_float2(1.f, 0.f) : twl[g * AY + k1];
       if (cc == 0) {
         constexpr int H = AY / 2;
         float2 a, b;
@@ -298,7 +302,7 @@ __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
 // memory (srow, NX floats); FUSE re-applies forward pass 0.
 template <class T, class Epi, bool FUSE, class Skip, bool COMPACT>
 __device__ __forceinline__ void x_last_staged(float2* sm, float* stg, Epi& epi, int z, int y0base,
-                                              const float2* __restrict__ tw, const Skip& skip,
+                                              const float2* tw, const Skip& skip,
                                               const int* nf, int L) {
   using X = typename T::X;
   constexpr int R = X::radix(0), span = X::span(0);
@@ -323,7 +327,7 @@ __device__ __forceinline__ void x_last_staged(float2* sm, float* stg, Epi& epi, 
     for (int t = 0; t < R; ++t) v[t] = row[xp<T>(i + t * span)];
     if (i != 0) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k]));
+      for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], tw[i * k]);
     }
     dft<R, +1>(v);
     float* srow = stg + r * T::NX;
@@ -334,7 +338,7 @@ __device__ __forceinline__ void x_last_staged(float2* sm, float* stg, Epi& epi, 
       dft<R, -1>(v);
       if (i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k]));
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], tw[i * k]);
       }
 #pragma unroll
       for (int t = 0; t < R; ++t) row[xp<T>(i + t * span)] = v[t];
@@ -406,6 +410,19 @@ __global__ void __launch_bounds__(256, 3)
       }
     }
   }
+  // twiddles into shared memory while the tile is in flight: the lines'
+  // y split factors w_ny^(y0*k1) (1 for k1 = 0 or y0 = 0) and, when they fit,
+  // the x table w_M^t
+  __shared__ float2 s_twl[X::TG * X::AY];
+  __shared__ float2 s_twx[X::TW_SMEM ? X::M : 1];
+  for (int t = threadIdx.x; t < X::TG * X::AY; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) {
+    const int g = t / X::AY, k1 = t - g * X::AY, y0 = y0base + g;
+    s_twl[t] = (k1 != 0 && y0 != 0) ? __ldg(&T.twny[y0 * k1]) : make_float2(1.f, 0.f);
+  }
+  if constexpr (X::TW_SMEM)
+    for (int t = threadIdx.x; t < X::M; t += CLARITY_BLOCK_STRIDE(SH::THREADS)) s_twx[t] = __ldg(&T.twx[t]);
+  const float2* twx = X::TW_SMEM ? s_twx : T.twx;
+  __syncthreads();
   bool ok = mbar_wait(&bars[0], 0, T.err);
   if (!ok) {
     mbar_wait(&bars[0], 0, nullptr);  // give copies in flight a last chance
@@ -416,14 +433,14 @@ __global__ void __launch_bounds__(256, 3)
   int L = SH::AY;
   if constexpr (Epi::has_zero_rows) L = epi.live_rows(y0base, SH::BY, SH::AY);
   constexpr bool CP = Epi::has_zero_rows;
-  cols_inverse_tma<SH>(buf, y0base, T.twr, T.twny, L);
+  cols_inverse_tma<SH>(buf, y0base, T.twr, s_twl, L);
   const RowSkip<TS, Epi> skip{epi, z, y0base};
-  x_inverse_down_to<TS, 1, RowSkip<TS, Epi>, CP>(buf, T.twx, skip, L);
+  x_inverse_down_to<TS, 1, RowSkip<TS, Epi>, CP>(buf, twx, skip, L);
   if (!mbar_wait(&bars[1], 0, T.err)) {
     mbar_wait(&bars[1], 0, nullptr);
     return;
   }
-  x_last_staged<TS, Epi, FUSE, RowSkip<TS, Epi>, CP>(buf, stg, epi, z, y0base, T.twx, skip,
+  x_last_staged<TS, Epi, FUSE, RowSkip<TS, Epi>, CP>(buf, stg, epi, z, y0base, twx, skip,
                                                      nf, L);
   if constexpr (Epi::kStoreRows) {
     // the epilogue's output rows, written in place of its input, leave by
@@ -454,8 +471,8 @@ __global__ void __launch_bounds__(256, 3)
       }
     }
     __syncthreads();
-    x_forward_from<TS, 1, RowSkip<TS, Epi>, CP>(buf, T.twx, skip, L);
-    cols_forward_tma<SH>(buf, y0base, T.twr, T.twny, L);
+    x_forward_from<TS, 1, RowSkip<TS, Epi>, CP>(buf, twx, skip, L);
+    cols_forward_tma<SH>(buf, y0base, T.twr, s_twl, L);
     fence_smem_to_async();
     __syncthreads();
     if (threadIdx.x == 0) {
