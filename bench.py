@@ -253,9 +253,9 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
                                                                 stream=stream))
         res["chosen"]["idiv"] = finals[k_acc]
         res["speedup"] = res["plain"]["ms"] / res["chosen"]["ms"]
-    # learned start (when trained weights are present): RL 5 iterations, the
-    # network's prediction, RL resumed from it (plain or accelerated) until
-    # the target is met
+    # learned start (when trained weights are present): RL to the iterate the
+    # network was trained on, the network's prediction, RL resumed from it
+    # (plain or accelerated) until the target is met
     from clarity_b200 import learned
     if os.path.exists(learned.WEIGHTS):
         net = learned.load_net()
@@ -269,9 +269,9 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
                 if float(tl[k].item()) <= target:
                     k_ls, ls_final = k, float(tl[k].item())
                     break
-            ls = {"form": "learned start (3-D U-Net on RL iterate 5, BF16 tensor-core kernels) "
-                          + ("+ accelerated RL" if accel else "+ resumed RL"),
-                  "pre_iterations": 5, "resumed_iterations": k_ls}
+            ls = {"form": f"learned start (3-D U-Net on RL iterate {net.pre}, BF16 tensor-core "
+                          "kernels) " + ("+ accelerated RL" if accel else "+ resumed RL"),
+                  "pre_iterations": net.pre, "resumed_iterations": k_ls}
             if k_ls:
                 ls["ms"] = ev_ms(lambda: learned.learned_solve(net, img_d, psf_d, out, k_ls,
                                                                stream=stream, accel=accel))

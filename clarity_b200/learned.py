@@ -10,7 +10,7 @@ advanced estimate, and RL resumes from it (clarityx_ml_ex_device with a start
 estimate); plain RL remains the fallback, and the I-divergence traces of
 both tell which is ahead.
 
-    python -m clarity_b200.learned --patches 2000 --epochs 6 --out weights.npy
+    python -m clarity_b200.learned --patches 2000 --epochs 14 --early 5 --out weights.npy
 """
 from __future__ import annotations
 
@@ -24,8 +24,15 @@ import numpy as np
 
 from . import api, synthetic as syn, unet
 
-WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_start_weights.npy")
+WEIGHTS = os.environ.get("CLARITY_LEARNED_WEIGHTS") or os.path.join(
+    os.path.dirname(os.path.abspath(__file__)), "learned_start_weights.npy")
 PATCH_ZYX = (48, 128, 128)
+PRE = 5  # RL iterations before the network, unless the weights' metadata says otherwise
+
+
+def meta_path(weights: str) -> str:
+    """The JSON file beside a weights file: {"pre": ..., "epochs": ..., "patches": ...}."""
+    return os.path.splitext(weights)[0] + ".json"
 
 
 def make_patch(seed: int, shape_zyx=PATCH_ZYX):
@@ -104,12 +111,15 @@ def train(net: unet.UNet3D, xe, xl, epochs: int = 6, lr: float = 1e-3, batch: in
     return hist
 
 
-def learned_solve(net: unet.UNet3D, img_d, psf_d, out, post: int, pre: int = 5,
+def learned_solve(net: unet.UNet3D, img_d, psf_d, out, post: int, pre: int | None = None,
                   idiv=None, stream=None, accel=False):
-    """RL `pre` iterations, the network's prediction, RL resumed for `post`
-    iterations from it -- plain, or accelerated (Biggs-Andrews) with accel
-    (idiv: trace of the resumed part, post + 1 entries)."""
+    """RL `pre` iterations (default: the iterate the network was trained on),
+    the network's prediction, RL resumed for `post` iterations from it --
+    plain, or accelerated (Biggs-Andrews) with accel (idiv: trace of the
+    resumed part, post + 1 entries)."""
     import torch
+    if pre is None:
+        pre = getattr(net, "pre", PRE)
     early = torch.empty_like(img_d)
     api.ml_device(img_d, psf_d, early, pre, stream)
     start = unet.predict(net, early, stream=stream).contiguous()
@@ -126,6 +136,10 @@ def learned_solve(net: unet.UNet3D, img_d, psf_d, out, post: int, pre: int = 5,
 def load_net(path: str = WEIGHTS) -> unet.UNet3D:
     net = unet.UNet3D()
     net.load_state(np.load(path))
+    net.pre = PRE
+    if os.path.exists(meta_path(path)):
+        with open(meta_path(path)) as f:
+            net.pre = int(json.load(f).get("pre", PRE))
     return net
 
 
@@ -136,6 +150,8 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--early", type=int, default=PRE,
+                    help="the RL iterate the network starts from")
     ap.add_argument("--log", default=None)
     a = ap.parse_args()
     logf = open(a.log, "w") if a.log else None
@@ -147,10 +163,12 @@ def main():
             logf.flush()
 
     api.register()
-    xe, xl = generate_pairs(a.patches, log=log)
+    xe, xl = generate_pairs(a.patches, early=a.early, log=log)
     net = unet.UNet3D(seed=1)
     hist = train(net, xe, xl, epochs=a.epochs, lr=a.lr, batch=a.batch, log=log)
     np.save(a.out, net.state())
+    with open(meta_path(a.out), "w") as f:
+        json.dump({"pre": a.early, "epochs": a.epochs, "patches": a.patches}, f)
     log(json.dumps({"losses": hist, "out": a.out}))
 
 
