@@ -191,8 +191,8 @@ def family_bytes(work, img_vox, ker_vox, iters):
 # DRAM bytes (read + write) per launch of each steady-iteration kernel family,
 # from the ncu capture of iteration 2 of this workload
 # (profiles/kernels_rl_iteration_512x512x128.md; z: mean of its two launches).
-NCU_TRAFFIC = {"xy_product": 152.1e6 + 215.3e6, "xy_inv_fwd": 84.5e6 + 19.4e6,
-               "z": (271.7e6 + 88.3e6 + 203.6e6 + 86.2e6) / 2}
+NCU_TRAFFIC = {"xy_product": 152.1e6 + 215.7e6, "xy_inv_fwd": 84.5e6 + 19.7e6,
+               "z": (270.7e6 + 46.4e6 + 203.5e6 + 86.7e6) / 2}
 
 
 def max_over_ranks(value, dist, device):
