@@ -155,7 +155,13 @@ int main(int argc, char** argv) {
     r = clarityx_convolve_noalloc(img.data(), id, psf.data(), kd, out.data(), nullptr);
   else if (op == "wiener")
     r = Clarity_WienerDeconvolve(img.data(), id, psf.data(), kd, out.data(), (float)param);
-  else
+  else if (op == "u16") {  // raw uint16 volumes (inputs hold integers); out = the uint16 result
+    std::vector<uint16_t> gi(ni), gk(nk), go(ni);
+    for (size_t i = 0; i < ni; ++i) gi[i] = (uint16_t)img[i];
+    for (size_t i = 0; i < nk; ++i) gk[i] = (uint16_t)psf[i];
+    r = clarityx_ml_u16(gi.data(), id, gk.data(), kd, go.data(), (int)param);
+    for (size_t i = 0; i < ni; ++i) out[i] = (float)go[i];
+  } else
     return 2;
   if (r != CLARITY_SUCCESS) {
     std::fprintf(stderr, "%s returned %d\n", op.c_str(), (int)r);

@@ -175,3 +175,15 @@ def test_emulated_specialised_box_with_uneven_split(emu, tmp_path, ishape, kshap
     assert rel_l2(run_emu(emu, tmp_path, "rl", img, psf, 3), oracle_lib.rl(img, psf, 3)) <= 2e-6
     out, _ = oracle_lib.rl_accel(img, psf, 2)
     assert rel_l2(run_emu(emu, tmp_path, "accel", img, psf, 2), out) <= 2e-6
+
+
+def test_emulated_u16_path_casts_like_x86(emu, tmp_path):
+    # the raw-volume entry point (device casts in, RL, device cast out)
+    # equals the float path's result cast as static_cast<unsigned short>
+    # does on x86: truncation, low 16 bits (values above 65535 wrap)
+    r = syn.rng(21)
+    img = r.integers(0, 60000, size=(12, 20, 24)).astype(np.float32)
+    psf = (syn.gaussian_psf((12, 20, 24), 1.5, 2.0) * 60000).astype(np.uint16).astype(np.float32)
+    ref = run_emu(emu, tmp_path, "rl", img, psf, 3).astype(np.float64)
+    v = np.trunc(ref).astype(np.int64) & 0xFFFF
+    assert np.array_equal(run_emu(emu, tmp_path, "u16", img, psf, 3), v.astype(np.float32))
