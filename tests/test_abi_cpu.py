@@ -110,6 +110,15 @@ def test_planner_invariants(work):
     assert p["xy_blocks"] == z * (p["By"] // p["G"])
 
 
+def test_benchmark_box_gets_the_specialised_tiling():
+    # the 512x512x128 box (256x256x64 image + same-size PSF) must plan exactly
+    # the compile-time shape its TMA XY pass and per-line Z pass are built for
+    # (x radices 16.16, Ay 16, y0 radices 8.4, z radices 16.8, G 2, W 2)
+    p = api.plan_info((128, 512, 512))
+    assert (p["M"], p["Ay"], p["By"], p["G"], p["W"]) == (256, 16, 32, 2, 2)
+    assert (p["x_passes"], p["y0_passes"], p["z_passes"]) == (2, 2, 2)
+
+
 def test_planner_rejects_unsupported_prime():
     with pytest.raises(api.ClarityError) as e:
         api.plan_info((8, 8, 2 * 23))
