@@ -490,11 +490,7 @@ struct ModOTF {
                         off + chunk <= total ? chunk : total - off);
   }
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
-#ifdef PROBE_NOH
-    const float2 h = make_float2(1.f, 1e-3f * (float)(idx & 7));
-#else
     const float2 h = __ldg(&H[idx]);
-#endif
     const float f = scale2 ? scale * *scale2 : scale;
     return make_float2(f * (v.x * h.x - v.y * h.y), f * (v.x * h.y + v.y * h.x));
   }
