@@ -85,6 +85,15 @@ static cudaEvent_t take_event() {
 // timing events are recorded into the capture.
 static thread_local bool t_capturing = false;
 void set_capturing(bool on) { t_capturing = on; }
+// Programmatic dependent launch of the steady RL passes: off while a graph is
+// captured and when CLARITY_PDL=0.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("CLARITY_PDL");
+    return !(v && v[0] == '0');
+  }();
+  return on && !t_capturing;
+}
 
 void note_launch_begin(int kind, cudaStream_t st) {
   g_launches.fetch_add(1);
@@ -291,6 +300,7 @@ static constexpr int kFinishThreads = 1024;
 __global__ void __launch_bounds__(kFinishThreads)
     k_finish_rl_scale(const double* partial, const int* np, const double* energy,
                       double* sum_out, float* scale_out) {
+  CLARITY_PDL_WAIT();  // the product pass's partials are complete and visible
   const double t = block_total(partial, *np);
   if (threadIdx.x == 0) {
     sum_out[0] = t;
@@ -918,7 +928,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
       // in the product pass itself cost more: each of its blocks then waited
       // for an atomic's round trip before it could exit.
       count_small();
-      CLARITY_LAUNCH(k_finish_rl_scale, 1, kFinishThreads, 0, st)(
+      CLARITY_LAUNCH_PDL(k_finish_rl_scale, 1, kFinishThreads, 0, st, pdl_enabled())(
           ws.partial, ws.iscal, ws.dscal + 0, ws.dscal + 1, sdev);
       CL_CHECK(cudaGetLastError());
     }
@@ -1085,7 +1095,7 @@ Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, D
     epi.nblocks = ws->iscal;
     CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
     count_small();
-    CLARITY_LAUNCH(k_finish_rl_scale, 1, kFinishThreads, 0, st)(
+    CLARITY_LAUNCH_PDL(k_finish_rl_scale, 1, kFinishThreads, 0, st, pdl_enabled())(
         ws->partial, ws->iscal, ws->dscal + 0, ws->dscal + 1, sdev);
     count_small();
     CLARITY_LAUNCH(k_accel_update, kReduceBlocks, 256, 0, st)(B[ui], Y, G, sdev, k == 0 ? 1 : 0,

@@ -173,6 +173,7 @@ void set_last_error(const char* msg);
 void note_launch_begin(int kind, cudaStream_t st);
 void note_launch_end(int kind, cudaStream_t st);
 void set_capturing(bool on);
+bool pdl_enabled();
 // cudaFuncSetAttribute(MaxDynamicSharedMemorySize) for kernels above 48 KB,
 // issued once per kernel, device and size (the attribute call is not free, and
 // a solve launches each kernel hundreds of times).

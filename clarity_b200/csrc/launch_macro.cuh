@@ -9,6 +9,44 @@
 #include <cuda_runtime.h>
 #define CLARITY_LAUNCH(kernel, grid, block, smem, stream) \
   kernel<<<(grid), (block), (smem), (stream)>>>
+namespace clarity {
+// Launch with programmatic stream serialisation when pdl is set: the grid may
+// be scheduled while the previous kernel on the stream drains its last
+// blocks, and every such kernel calls pdl_wait() before it touches memory,
+// which returns once the previous grid has completed and its writes are
+// visible.  Without pdl this is an ordinary launch.
+template <class... P>
+struct PdlLauncher {
+  void (*k)(P...);
+  dim3 grid, block;
+  size_t smem;
+  cudaStream_t st;
+  bool pdl;
+  template <class... A>
+  void operator()(A&&... args) const {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    (void)cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(args)...);
+  }
+};
+template <class... P>
+inline PdlLauncher<P...> pdl_launcher(void (*k)(P...), dim3 grid, dim3 block, size_t smem,
+                                      cudaStream_t st, bool pdl) {
+  return PdlLauncher<P...>{k, grid, block, smem, st, pdl};
+}
+}  // namespace clarity
+#define CLARITY_LAUNCH_PDL(kernel, grid, block, smem, stream, pdl) \
+  ::clarity::pdl_launcher((kernel), dim3(grid), dim3(block), (smem), (stream), (pdl))
+// First statement of a kernel launched by CLARITY_LAUNCH_PDL.
+#define CLARITY_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
 #define CLARITY_DYN_SMEM(T, name) extern __shared__ __align__(128) T name[]
 // Loop stride of a block-wide strided loop in kernels launched with a
 // compile-time block size.
@@ -19,6 +57,9 @@
 #include "emu_cuda.hpp"
 #define CLARITY_LAUNCH(kernel, grid, block, smem, stream) \
   ::clarity_emu::launcher((grid), (smem))(kernel)
+#define CLARITY_LAUNCH_PDL(kernel, grid, block, smem, stream, pdl) \
+  ::clarity_emu::launcher((grid), (smem))(kernel)
+#define CLARITY_PDL_WAIT() ((void)0)
 #define CLARITY_DYN_SMEM(T, name) T* name = ::clarity_emu::dynamic_smem<T>()
 #define CLARITY_BLOCK_STRIDE(n) ((int)blockDim.x)
 #define CLARITY_ISSUE_LANES ((int)blockDim.x)

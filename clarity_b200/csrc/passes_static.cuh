@@ -747,6 +747,7 @@ template <class SH, class Mod>
 __global__ void __launch_bounds__(256, 2)
     ks_z2(const Mod mod, const float2* __restrict__ Sin, float2* __restrict__ Sout,
           const Tables T) {
+  CLARITY_PDL_WAIT();  // the previous kernel's output is complete and visible
   CLARITY_DYN_SMEM(float2, sm);
   static_assert(SH::Y_PER_LINE, "y0 per-line Z kernel needs BY <= 32");
   constexpr int BY = SH::BY, W = SH::W, BW = SH::BW, NZ = SH::NZ, ZS = SH::ZS;

@@ -352,6 +352,7 @@ __device__ __forceinline__ void x_last_staged(float2* sm, float* stg, Epi& epi, 
 template <class SH, class Epi, bool FUSE>
 __global__ void __launch_bounds__(256, 3)
     ks_xy_tma(Epi epi, CLARITY_GRID_CONST TensorMap tm, const Tables T) {
+  CLARITY_PDL_WAIT();  // the previous pass's output is complete and visible
   using X = XyTma<SH>;
   using TS = typename X::T;
   static_assert(X::OK, "shape not supported by the TMA XY pass");

@@ -85,7 +85,7 @@ inline bool try_xy_tma(const PlanEntry& pe, cudaStream_t st, const F& fn, const 
     const int blocks = nz * (SH::BY / X::TG);
     if (blocks <= 0) return true;
     note_launch_begin(family, st);
-    CLARITY_LAUNCH(k, blocks, SH::THREADS, X::SMEM, st)(fn, tm, T);
+    CLARITY_LAUNCH_PDL(k, blocks, SH::THREADS, X::SMEM, st, pdl_enabled())(fn, tm, T);
     note_launch_end(family, st);
     *err = cudaGetLastError();
     return true;
@@ -120,7 +120,8 @@ inline bool try_static(const PlanEntry& pe, cudaStream_t st, const F& fn, float2
       *err = allow_smem_st(k, SH::Z2_SMEM);
       if (*err != cudaSuccess) return true;
       note_launch_begin(KK_Z, st);
-      CLARITY_LAUNCH(k, pe.P.z_blocks, SH::THREADS, SH::Z2_SMEM, st)(fn, Sb, Sa, T);
+      CLARITY_LAUNCH_PDL(k, pe.P.z_blocks, SH::THREADS, SH::Z2_SMEM, st, pdl_enabled())(fn, Sb,
+                                                                                     Sa, T);
       note_launch_end(KK_Z, st);
     } else {
       auto k = st::ks_z<SH, F>;
