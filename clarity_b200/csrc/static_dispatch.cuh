@@ -20,6 +20,11 @@ using ShapeW128 = st::Shape<st::Rad<8, 8>, 16, st::Rad<8>, st::Rad<8, 8>, 1, 4>;
 using ShapeW1024 = st::Shape<st::Rad<8, 8, 8>, 16, st::Rad<8, 8>, st::Rad<16, 16>, 2, 1>;
 using ShapeW64 = st::Shape<st::Rad<8, 4>, 16, st::Rad<4>, st::Rad<8, 4>, 4, 1>;
 
+// The 512x512x128 box keeps its TMA XY pass with shared-memory twiddles and
+// three blocks per SM; a tile change that breaks this fails to compile.
+static_assert(st::XyTma<ShapeW512>::OK && st::XyTma<ShapeW512>::TW_SMEM,
+              "the 512x512x128 XY tile no longer fits three TMA blocks per SM");
+
 template <class... SHs>
 struct ShapeList {};
 using StaticShapes = ShapeList<ShapeW512, ShapeW128, ShapeW1024, ShapeW64>;
