@@ -58,6 +58,7 @@ EXTENSION_SYMBOLS = [
     "clarityx_convolve_noalloc", "clarityx_ml_batch_device", "clarityx_autotune",
     "clarityx_ml_ex_device", "clarityx_ml_accel_device", "clarityx_ml_u16",
     "clarityx_blind_ml_psf_device",
+    "clarityx_idiv_deconvolve_device",
     "clarityx_nn_conv3", "clarityx_nn_conv3_wgrad", "clarityx_nn_conv_in",
     "clarityx_nn_conv_in_wgrad", "clarityx_nn_head", "clarityx_nn_head_loss_grad",
     "clarityx_nn_pool2", "clarityx_nn_merge_skip_grad", "clarityx_nn_up_grad",
@@ -157,6 +158,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_ml_u16.restype = i
         L.clarityx_blind_ml_psf_device.argtypes = [vp, Dim3, vp, Dim3, vp, vp, i, i, vp]
         L.clarityx_blind_ml_psf_device.restype = i
+        L.clarityx_idiv_deconvolve_device.argtypes = [vp, Dim3, vp, Dim3, vp, i, C.c_float, vp]
+        L.clarityx_idiv_deconvolve_device.restype = i
         L.clarityx_autotune.argtypes = [i]
         L.clarityx_autotune.restype = None
         L.clarityx_launch_count.restype = C.c_longlong
@@ -452,6 +455,13 @@ def maximum_likelihood_deconvolve_u16(image, kernel, iterations: int) -> np.ndar
     out = np.empty_like(image)
     _check(load().clarityx_ml_u16(image, dim3(image), kernel, dim3(kernel), out, int(iterations)))
     return out
+
+
+def idiv_deconvolve_device(image, kernel, out, iterations, alpha=0.0, stream=None):
+    """clarityx_idiv_deconvolve_device: I-divergence restoration
+    (Markham-Conchello conjugate gradients on s = a^2)."""
+    return _dev("clarityx_idiv_deconvolve_device", image, kernel, out,
+                [int(iterations), C.c_float(float(alpha))], stream)
 
 
 def blind_ml_psf_device(image, kernel, out, iterations, psf_subiterations=5, psf_out=None,

@@ -409,6 +409,19 @@ ClarityResult_t clarityx_ml_device(const float* image, Clarity_Dim3 imageDim,
                      });
 }
 
+ClarityResult_t clarityx_idiv_deconvolve_device(const float* image, Clarity_Dim3 imageDim,
+                                               const float* kernel, Clarity_Dim3 kernelDim,
+                                               float* out, int iterations, float alpha,
+                                               void* stream) {
+  if (iterations < 0) return fail(CLARITY_INVALID_ARGUMENT, "iterations < 0");
+  if (!(alpha >= 0.f)) return fail(CLARITY_INVALID_ARGUMENT, "alpha < 0 or NaN");
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_idiv_cg(c, i, id, k, kd, o, iterations, alpha);
+                     });
+}
+
 ClarityResult_t clarityx_blind_ml_psf_device(const float* image, Clarity_Dim3 imageDim,
                                              const float* kernel, Clarity_Dim3 kernelDim,
                                              float* out, float* psf_out, int iterations,

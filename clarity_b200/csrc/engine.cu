@@ -444,6 +444,7 @@ static void free_workspace(Workspace& w) {
   cudaFree(w.partial); cudaFree(w.dscal); cudaFree(w.fscal); cudaFree(w.iscal);
   cudaFree(w.HG);
   for (float* b : w.accel) cudaFree(b);
+  for (float* b : w.xbuf) cudaFree(b);
   w = Workspace();
 }
 
@@ -1295,6 +1296,289 @@ Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
 // PSF step deconvolves by the object (its spectrum as the OTF) and rescales
 // to 1.  The object and PSF estimates live on the work box; psf_out (optional)
 // receives the PSF on the kernel's grid.
+// ------------------------------------------------- I-divergence restoration
+// Markham and Conchello (J. Opt. Soc. Am. A 18(5), 2001), the method the
+// reference declares (Clarity.h.in:294-319) and leaves a stub
+// (src/IDivergenceDeconvolve.cxx).  Minimises sum g ln(g/gh) + gh - g +
+// alpha sum s^2 over the work box (g zero-padded, gh = h * s) with s = a^2,
+// by Polak-Ribiere conjugate gradients on a; the step solves dJ/dl = 0 by
+// kIdivNewton Newton steps on the exact quadratic gh(l) = gh + l h*(2ad) +
+// l^2 h*(dd).  Per-voxel line-search terms and all sums in FP64.
+static constexpr int kIdivNewton = 4;
+
+__device__ __forceinline__ double idiv_ratio(double g, double b) { return b > 1e-5 ? g / b : 0.0; }
+
+// a = sqrt(g) on the work box (g zero-padded)
+__global__ void k_idiv_start(ImageSrc g, WorkVol w, float* __restrict__ a) {
+  const long long n = (long long)w.nx * w.ny * w.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % w.nx);
+    const long long r = i / w.nx;
+    const float v = g.at(x, (int)(r % w.ny), (int)(r / w.ny));
+    a[i] = sqrtf(v > 0.f ? v : 0.f);
+  }
+}
+
+// t = c * a * b (b == nullptr: c * a * a)
+__global__ void k_idiv_prod(const float* __restrict__ a, const float* __restrict__ b, float c,
+                            float* __restrict__ t, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float bv = b ? b[i] : a[i];
+    t[i] = c == 1.f ? a[i] * bv : c * a[i] * bv;
+  }
+}
+
+// t = 1 - g / gh (the ratio 0 where gh <= 1e-5)
+__global__ void k_idiv_resid(ImageSrc g, WorkVol w, const float* __restrict__ gh,
+                             float* __restrict__ t) {
+  const long long n = (long long)w.nx * w.ny * w.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % w.nx);
+    const long long r = i / w.nx;
+    const float gv = g.at(x, (int)(r % w.ny), (int)(r / w.ny));
+    t[i] = (float)(1.0 - idiv_ratio(gv, gh[i]));
+  }
+}
+
+// grn = 2 a (q + 2 alpha a^2)
+__global__ void k_idiv_grad(const float* __restrict__ a, const float* __restrict__ q, float alpha2,
+                            float* __restrict__ grn, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float av = a[i];
+    grn[i] = 2.f * av * (q[i] + alpha2 * av * av);
+  }
+}
+
+// d = -gr (first direction)
+__global__ void k_idiv_negate(const float* __restrict__ gr, float* __restrict__ d, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    d[i] = -gr[i];
+}
+
+// FP64 sums of dJ/dl and d2J/dl2 at l = *lam (partial[b], partial[nb + b])
+__global__ void k_idiv_newton_sums(ImageSrc g, WorkVol w, const float* __restrict__ gh,
+                                   const float* __restrict__ p1, const float* __restrict__ p2,
+                                   const float* __restrict__ a, const float* __restrict__ d,
+                                   const double* __restrict__ lam, double alpha,
+                                   double* __restrict__ partial) {
+  const long long n = (long long)w.nx * w.ny * w.nz;
+  const double l = *lam;
+  double f1 = 0, f2 = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % w.nx);
+    const long long r = i / w.nx;
+    const double gv = g.at(x, (int)(r % w.ny), (int)(r / w.ny));
+    const double q2 = p2[i];
+    const double ghl = (double)gh[i] + l * (double)p1[i] + l * l * q2;
+    const double gp = (double)p1[i] + 2.0 * l * q2;
+    const double rr = idiv_ratio(gv, ghl);
+    f1 += (1.0 - rr) * gp;
+    f2 += (ghl > 1e-5 ? rr / ghl : 0.0) * gp * gp + (1.0 - rr) * 2.0 * q2;
+    const double dd = d[i], sl = (double)a[i] + l * dd;
+    f1 += 4.0 * alpha * sl * sl * sl * dd;
+    f2 += 12.0 * alpha * sl * sl * dd * dd;
+  }
+  block_sum_store(f1, partial + 0 * gridDim.x);
+  block_sum_store(f2, partial + 1 * gridDim.x);
+}
+
+// one Newton step: l <- max(0, l - f1/f2) when f2 > 0
+__global__ void k_idiv_newton_finish(const double* partial, int np, double* lam) {
+  const double f1 = block_total(partial, np);
+  __syncthreads();
+  const double f2 = block_total(partial + np, np);
+  if (threadIdx.x == 0 && f2 > 0) {
+    double l = *lam - f1 / f2;
+    *lam = l < 0 ? 0 : l;
+  }
+}
+
+// a += l d, gh += l p1 + l^2 p2
+__global__ void k_idiv_move(float* __restrict__ a, const float* __restrict__ d,
+                            float* __restrict__ gh, const float* __restrict__ p1,
+                            const float* __restrict__ p2, const double* __restrict__ lam,
+                            long long n) {
+  const double l = *lam;
+  const float lf = (float)l, l2 = (float)(l * l);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    a[i] = a[i] + lf * d[i];
+    gh[i] = gh[i] + lf * p1[i] + l2 * p2[i];
+  }
+}
+
+// Polak-Ribiere sums: grn . (grn - gr) and gr . gr
+__global__ void k_idiv_pr_sums(const float* __restrict__ grn, const float* __restrict__ gr,
+                               long long n, double* __restrict__ partial) {
+  double s1 = 0, s2 = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double a = grn[i], b = gr[i];
+    s1 += a * (a - b);
+    s2 += b * b;
+  }
+  block_sum_store(s1, partial + 0 * gridDim.x);
+  block_sum_store(s2, partial + 1 * gridDim.x);
+}
+
+// beta = max(0, s1 / s2); d = -grn + beta d; gr = grn.  The sums are
+// finished by every block (fixed order, identical results), so one launch
+// both finishes and applies them.
+__global__ void k_idiv_direction(const double* partial, int np, float* __restrict__ d,
+                                 const float* __restrict__ grn, float* __restrict__ gr,
+                                 long long n) {
+  __shared__ float sbeta;
+  const double s1 = block_total(partial, np);
+  __syncthreads();
+  const double s2 = block_total(partial + np, np);
+  if (threadIdx.x == 0) {
+    double b = s2 > 0 ? s1 / s2 : 0.0;
+    sbeta = (float)(b < 0 ? 0 : b);
+  }
+  __syncthreads();
+  const float beta = sbeta;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gn = grn[i];
+    d[i] = -gn + beta * d[i];
+    gr[i] = gn;
+  }
+}
+
+// v <- h (x) v on the work box (in place): forward transform, the spectral
+// product with `otf` (H for a convolution, conj(H) for a correlation) and 1/N,
+// inverse transform.
+static Status conv_work(Context& ctx, const PlanEntry& pe, Workspace& ws, const float2* otf,
+                        float* v, Dims wd) {
+  const VolPlan& P = pe.P;
+  const WorkVol wv{wd.x, wd.y, wd.z};
+  CL_TRY(xy_forward(ctx, pe, ProWork{v, nullptr, wv, P.xmode}, ws.S));
+  CL_TRY(z_pass(ctx, pe, ModOTF{otf, inv_volume(wd)}, ws.S, ws.S));
+  CL_TRY(xy_inverse(ctx, pe, EpiWork{v, wv, P.xmode}, ws.S));
+  return Status::Ok();
+}
+
+__global__ void k_conj_spectrum(const float2* __restrict__ h, float2* __restrict__ hc,
+                                long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float2 v = h[i];
+    hc[i] = make_float2(v.x, -v.y);
+  }
+}
+
+Status run_idiv_cg(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                   float* out, int iters, float alpha) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  cudaStream_t st = ctx.exec_stream();
+  const long long n = wd.n();
+  if (ws->accel_cap < n) {
+    for (float*& b : ws->accel) {
+      cudaFree(b);
+      b = nullptr;
+    }
+    ws->accel_cap = 0;
+    for (float*& b : ws->accel) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
+    ws->accel_cap = n;
+  }
+  if (ws->xbuf_cap < n) {
+    for (float*& b : ws->xbuf) {
+      cudaFree(b);
+      b = nullptr;
+    }
+    ws->xbuf_cap = 0;
+    for (float*& b : ws->xbuf) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
+    ws->xbuf_cap = n;
+  }
+  {
+    long long pc = ws->partial_cap;
+    CL_TRY(ensure(&ws->partial, &pc, 2 * (long long)kReduceBlocks));
+    ws->partial_cap = (int)pc;
+  }
+  if (!ws->HG) CL_CHECK(dev_alloc((void**)&ws->HG, sizeof(float2) * (size_t)ws->spec_cap));
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  count_small();
+  CLARITY_LAUNCH(k_conj_spectrum, kReduceBlocks, 256, 0, st)(ws->H, ws->HG, pe->P.spec_elems);
+  CL_CHECK(cudaGetLastError());
+  const ImageSrc g = image_src(img, id);
+  const WorkVol wv{wd.x, wd.y, wd.z};
+  float* a = ws->accel[0];
+  float* d = ws->accel[1];
+  float* gr = ws->accel[2];
+  float* grn = ws->accel[3];
+  float* gh = ws->accel[4];
+  float* p1 = ws->xbuf[0];
+  float* p2 = ws->xbuf[1];
+  float* t = ws->u;
+  double* lam = ws->dscal + 4;
+  const float alpha2 = 2.f * alpha;
+  auto gradient = [&]() -> Status {
+    count_small();
+    CLARITY_LAUNCH(k_idiv_resid, kReduceBlocks, 256, 0, st)(g, wv, gh, t);
+    CL_CHECK(cudaGetLastError());
+    CL_TRY(conv_work(ctx, *pe, *ws, ws->HG, t, wd));
+    count_small();
+    CLARITY_LAUNCH(k_idiv_grad, kReduceBlocks, 256, 0, st)(a, t, alpha2, grn, n);
+    CL_CHECK(cudaGetLastError());
+    return Status::Ok();
+  };
+  count_small();
+  CLARITY_LAUNCH(k_idiv_start, kReduceBlocks, 256, 0, st)(g, wv, a);
+  count_small();
+  CLARITY_LAUNCH(k_idiv_prod, kReduceBlocks, 256, 0, st)(a, nullptr, 1.f, gh, n);
+  CL_CHECK(cudaGetLastError());
+  CL_TRY(conv_work(ctx, *pe, *ws, ws->H, gh, wd));
+  CL_TRY(gradient());
+  CL_CHECK(cudaMemcpyAsync(gr, grn, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+  count_small();
+  CLARITY_LAUNCH(k_idiv_negate, kReduceBlocks, 256, 0, st)(grn, d, n);
+  CL_CHECK(cudaGetLastError());
+  for (int k = 0; k < iters; ++k) {
+    count_small();
+    CLARITY_LAUNCH(k_idiv_prod, kReduceBlocks, 256, 0, st)(a, d, 2.f, p1, n);
+    CL_CHECK(cudaGetLastError());
+    CL_TRY(conv_work(ctx, *pe, *ws, ws->H, p1, wd));
+    count_small();
+    CLARITY_LAUNCH(k_idiv_prod, kReduceBlocks, 256, 0, st)(d, nullptr, 1.f, p2, n);
+    CL_CHECK(cudaGetLastError());
+    CL_TRY(conv_work(ctx, *pe, *ws, ws->H, p2, wd));
+    CL_CHECK(cudaMemsetAsync(lam, 0, sizeof(double), st));
+    for (int m = 0; m < kIdivNewton; ++m) {
+      count_small();
+      CLARITY_LAUNCH(k_idiv_newton_sums, kReduceBlocks, 256, 0, st)(g, wv, gh, p1, p2, a, d, lam,
+                                                                    (double)alpha, ws->partial);
+      count_small();
+      CLARITY_LAUNCH(k_idiv_newton_finish, 1, 256, 0, st)(ws->partial, kReduceBlocks, lam);
+      CL_CHECK(cudaGetLastError());
+    }
+    count_small();
+    CLARITY_LAUNCH(k_idiv_move, kReduceBlocks, 256, 0, st)(a, d, gh, p1, p2, lam, n);
+    CL_CHECK(cudaGetLastError());
+    CL_TRY(gradient());
+    count_small();
+    CLARITY_LAUNCH(k_idiv_pr_sums, kReduceBlocks, 256, 0, st)(grn, gr, n, ws->partial);
+    count_small();
+    CLARITY_LAUNCH(k_idiv_direction, kReduceBlocks, 256, 0, st)(ws->partial, kReduceBlocks, d, grn,
+                                                                gr, n);
+    CL_CHECK(cudaGetLastError());
+  }
+  count_small();
+  CLARITY_LAUNCH(k_idiv_prod, kReduceBlocks, 256, 0, st)(a, nullptr, 1.f, t, n);
+  count_small();
+  CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(t, wd.x, wd.y, out, id.x, id.y, id.z, nullptr);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
 Status run_blind_psf(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
                      float* out, float* psf_out, int iters, int psf_subiters) {
   const PlanEntry* pe;

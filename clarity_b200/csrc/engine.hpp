@@ -60,6 +60,8 @@ struct Workspace {
   int* iscal = nullptr;    // [0] number of partial sums the last product pass wrote
   float* accel[5] = {};    // accelerated RL: three estimates, extrapolated point, step
   long long accel_cap = 0;
+  float* xbuf[2] = {};     // I-divergence restoration: two more work-box volumes
+  long long xbuf_cap = 0;
   size_t img_cap = 0, ker_cap = 0;
   long long spec_cap = 0, work_cap = 0;
   int partial_cap = 0;
@@ -140,6 +142,10 @@ Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims
 // run_rl_ex (entries k < iters at the extrapolated points).
 Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
                     const float* start, float* out, int iters, double* idiv);
+// I-divergence restoration after Markham and Conchello (conjugate gradients
+// on s = a^2 with an exact quadratic line model); alpha weights sum s^2.
+Status run_idiv_cg(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                   float* out, int iters, float alpha);
 // Blind ML with the PSF update (alternating object and PSF steps; psf_out
 // optional, on the kernel's grid).
 Status run_blind_psf(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,

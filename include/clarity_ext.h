@@ -56,6 +56,18 @@ CLARITY_API ClarityResult_t clarityx_blind_ml_psf_device(
     Clarity_Dim3 kernelDim, float *out, float *psf_out, int iterations,
     int psf_subiterations, void *stream);
 
+/* I-divergence restoration after J. Markham and J.A. Conchello, J. Opt. Soc.
+ * Am. A 18(5), 2001: the method Clarity_IDivergenceDeconvolve declares
+ * (Clarity.h.in:294-319), whose reference body is a stub that writes zeros
+ * (src/IDivergenceDeconvolve.cxx).  Minimises sum g ln(g/gh) + gh - g +
+ * alpha sum s^2 with gh = kernel * s over the padded work box, s = a^2 >= 0,
+ * by `iterations` Polak-Ribiere conjugate-gradient steps on a from
+ * a = sqrt(image), each with an exact quadratic line model and four Newton
+ * steps.  alpha >= 0.  Device pointers, asynchronous on `stream`. */
+CLARITY_API ClarityResult_t clarityx_idiv_deconvolve_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, int iterations, float alpha, void *stream);
+
 /* Clarity_MaximumLikelihoodDeconvolve on uint16 host volumes, as the
  * reference's DeconvolveRawImages app does around it
  * (apps/DeconvolveRawImages/DeconvolveRawImages.cxx:91-116), with the casts on

@@ -97,6 +97,9 @@ class Oracle:
             fn = getattr(L, f"oracle_blind_psf_{pr}")
             fn.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, _f32p, i, i]
             fn.restype = None
+        for p in ("f32", "f64"):
+            getattr(L, f"oracle_idiv_cg_{p}").argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p,
+                                                         i, C.c_double]
         L.oracle_idivergence.argtypes = [_f32p, _f32p, C.c_long, C.POINTER(C.c_long)]
         L.oracle_idivergence.restype = C.c_double
         L.oracle_pad_shift.argtypes = [_f32p, i, i, i, _f32p, i, i, i,
@@ -173,6 +176,17 @@ class Oracle:
         getattr(self.lib, f"oracle_blind_psf_{precision}")(img, ix, iy, iz, psf, kx, ky, kz, out,
                                                            pout, int(iters), int(sub))
         return out, pout
+
+    def idiv_cg(self, img, psf, iters, alpha=0.0, precision="f32"):
+        """I-divergence restoration (Markham-Conchello conjugate gradients on
+        s = a^2); returns the estimate on the image region."""
+        img, psf = _f32(img), _f32(psf)
+        out = np.empty_like(img)
+        ix, iy, iz = _dims(img)
+        kx, ky, kz = _dims(psf)
+        getattr(self.lib, f"oracle_idiv_cg_{precision}")(img, ix, iy, iz, psf, kx, ky, kz, out,
+                                                         int(iters), float(alpha))
+        return out
 
     def wiener(self, img, psf, eps, precision="f32", work=False):
         return self._run("wiener", img, psf, [eps], precision, work)

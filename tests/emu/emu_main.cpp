@@ -155,6 +155,9 @@ int main(int argc, char** argv) {
     r = clarityx_convolve_noalloc(img.data(), id, psf.data(), kd, out.data(), nullptr);
   else if (op == "wiener")
     r = Clarity_WienerDeconvolve(img.data(), id, psf.data(), kd, out.data(), (float)param);
+  else if (op == "idiv" || op == "idiva")  // I-divergence restoration, alpha 0 or 1e-4
+    r = clarityx_idiv_deconvolve_device(img.data(), id, psf.data(), kd, out.data(), (int)param,
+                                        op == "idiva" ? 1e-4f : 0.f, nullptr);
   else if (op == "u16") {  // raw uint16 volumes (inputs hold integers); out = the uint16 result
     std::vector<uint16_t> gi(ni), gk(nk), go(ni);
     for (size_t i = 0; i < ni; ++i) gi[i] = (uint16_t)img[i];

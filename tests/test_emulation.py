@@ -187,3 +187,16 @@ def test_emulated_u16_path_casts_like_x86(emu, tmp_path):
     ref = run_emu(emu, tmp_path, "rl", img, psf, 3).astype(np.float64)
     v = np.trunc(ref).astype(np.int64) & 0xFFFF
     assert np.array_equal(run_emu(emu, tmp_path, "u16", img, psf, 3), v.astype(np.float32))
+
+
+@pytest.mark.parametrize("case,op,alpha", [("small_even", "idiv", 0.0), ("small_odd", "idiva", 1e-4)])
+def test_emulated_idiv_restoration_matches_oracle(emu, tmp_path, oracle_lib, case, op, alpha):
+    # the Markham-Conchello I-divergence restoration: the library's passes and
+    # reductions against the oracle's restatement of the same steps
+    d = load_golden(case)
+    img, psf = d["image"], d["psf"]
+    for iters in (1, 4):
+        got = run_emu(emu, tmp_path, op, img, psf, iters)
+        ref64 = oracle_lib.idiv_cg(img, psf, iters, alpha, precision="f64")
+        ref32 = oracle_lib.idiv_cg(img, psf, iters, alpha)
+        assert rel_l2(got, ref64) <= max(2e-6, 4 * rel_l2(ref32, ref64))

@@ -370,3 +370,23 @@ def test_blind_ml_psf_update_vs_oracle(clarity_gpu, oracle_lib, case, outer, sub
     torch.cuda.synchronize()
     assert rel_l2(out.cpu().numpy(),
                   clarity_gpu.blind_maximum_likelihood_deconvolve(img, psf, outer)) <= 1e-5
+
+
+@pytest.mark.parametrize("case,alpha", [("small_even", 0.0), ("cfg0_rl10", 1e-4)])
+def test_idiv_restoration_vs_oracle(clarity_gpu, oracle_lib, case, alpha):
+    # the Markham-Conchello I-divergence restoration (the reference declares
+    # it and ships a stub): the GPU solve against the oracle's restatement,
+    # held to the FP64 oracle at max(1e-5, four times the FP32 oracle's drift)
+    import torch
+    d = load_golden(case)
+    img, psf = d["image"], d["psf"]
+    di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
+    out = torch.empty_like(di)
+    for iters in (1, 4):
+        clarity_gpu.idiv_deconvolve_device(di, dk, out, iters, alpha=alpha)
+        torch.cuda.synchronize()
+        ref64 = oracle_lib.idiv_cg(img, psf, iters, alpha, precision="f64")
+        ref32 = oracle_lib.idiv_cg(img, psf, iters, alpha)
+        got = out.cpu().numpy()
+        assert np.all(got >= 0)
+        assert rel_l2(got, ref64) <= max(1e-5, 4 * rel_l2(ref32, ref64))
