@@ -138,3 +138,34 @@ def test_idivergence_oracle(oracle_lib):
     gh = np.array([1.0, 1.0, 0.5, 3.0], np.float32)
     want = 2 * np.log(2.0) + 1.0 - 2.0 + 0.5
     assert abs(oracle_lib.idivergence(g, gh) - want) < 1e-12
+
+
+def test_idiv_restoration_lowers_its_objective(oracle_lib):
+    # the Markham-Conchello restatement: the work-box objective
+    # sum g ln(g/gh) + gh - g + alpha sum s^2 (g zero-padded, gh = h * s, circular
+    # on the padded box) falls with every conjugate-gradient step, and s >= 0
+    d = load_golden("small_even")
+    img, psf = d["image"].astype(np.float64), d["psf"].astype(np.float64)
+    Z, Y, X = img.shape
+    kz, ky, kx = psf.shape
+    W = (Z + kz, Y + ky, X + kx)
+    g = np.zeros(W)
+    g[:Z, :Y, :X] = img
+    h = np.zeros(W)
+    h[:kz, :ky, :kx] = psf
+    H = np.fft.rfftn(np.roll(h, (-(kz // 2), -(ky // 2), -(kx // 2)), (0, 1, 2)))
+
+    def objective(est, alpha):
+        s = np.zeros(W)
+        s[:Z, :Y, :X] = est
+        gh = np.fft.irfftn(np.fft.rfftn(s) * H, W, axes=(0, 1, 2))
+        m = g > 0
+        return float((g[m] * np.log(g[m] / gh[m])).sum() + gh.sum() - g.sum()
+                     + alpha * (s ** 2).sum())
+
+    for alpha in (0.0, 1e-4):
+        ests = [oracle_lib.idiv_cg(d["image"], d["psf"], it, alpha, precision="f64")
+                for it in (0, 1, 2, 4, 8)]
+        js = [objective(e, alpha) for e in ests]
+        assert all(b < a for a, b in zip(js, js[1:])), js
+        assert all(e.min() >= 0 for e in ests)
