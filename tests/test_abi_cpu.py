@@ -83,6 +83,19 @@ def test_argument_errors_without_device():
     assert f32p is not None
 
 
+def test_idiv_restoration_argument_errors_without_device():
+    # iterations < 0 and a negative or NaN penalty are rejected before any
+    # device work, with the reason in clarityx_last_error
+    L = api.load()
+    d3 = api.Dim3(4, 4, 4)
+    for iters, alpha, word in ((-1, 0.0, "iterations"), (2, -1.0, "alpha"),
+                               (2, float("nan"), "alpha")):
+        rc = L.clarityx_idiv_deconvolve_device(C.c_void_p(16), d3, C.c_void_p(16), d3,
+                                               C.c_void_p(16), iters, C.c_float(alpha), None)
+        assert rc == api.CLARITY_INVALID_ARGUMENT
+        assert word in L.clarityx_last_error().decode()
+
+
 @pytest.mark.skipif(gpu_available(), reason="a GPU is present")
 def test_register_without_gpu_is_invalid_operation():
     code = api.load().Clarity_Register()
