@@ -567,6 +567,20 @@ static Status ensure(T** p, long long* cap, long long need) {
   return Status::Ok();
 }
 
+// A set of work-box volumes of at least n floats each (reallocated together).
+template <int K>
+static Status ensure_volumes(float* (&bufs)[K], long long* cap, long long n) {
+  if (*cap >= n) return Status::Ok();
+  for (float*& b : bufs) {
+    cudaFree(b);
+    b = nullptr;
+  }
+  *cap = 0;
+  for (float*& b : bufs) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
+  *cap = n;
+  return Status::Ok();
+}
+
 static Status fill_workspace(Workspace& w, const PlanEntry& pe, const Dims& img,
                              const Dims& ker);
 
@@ -1034,15 +1048,7 @@ Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, D
   }
   const VolPlan& P = pe->P;
   const long long n = wd.n();
-  if (ws->accel_cap < n) {
-    for (float*& b : ws->accel) {
-      cudaFree(b);
-      b = nullptr;
-    }
-    ws->accel_cap = 0;
-    for (float*& b : ws->accel) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
-    ws->accel_cap = n;
-  }
+  CL_TRY(ensure_volumes(ws->accel, &ws->accel_cap, n));
   // partials: one per XY block for the flux sum, two per reduce block for
   // the extrapolation sums
   {
@@ -1481,24 +1487,8 @@ Status run_idiv_cg(Context& ctx, const float* img, Dims id, const float* ker, Di
   CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
   cudaStream_t st = ctx.exec_stream();
   const long long n = wd.n();
-  if (ws->accel_cap < n) {
-    for (float*& b : ws->accel) {
-      cudaFree(b);
-      b = nullptr;
-    }
-    ws->accel_cap = 0;
-    for (float*& b : ws->accel) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
-    ws->accel_cap = n;
-  }
-  if (ws->xbuf_cap < n) {
-    for (float*& b : ws->xbuf) {
-      cudaFree(b);
-      b = nullptr;
-    }
-    ws->xbuf_cap = 0;
-    for (float*& b : ws->xbuf) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
-    ws->xbuf_cap = n;
-  }
+  CL_TRY(ensure_volumes(ws->accel, &ws->accel_cap, n));
+  CL_TRY(ensure_volumes(ws->xbuf, &ws->xbuf_cap, n));
   {
     long long pc = ws->partial_cap;
     CL_TRY(ensure(&ws->partial, &pc, 2 * (long long)kReduceBlocks));
@@ -1588,15 +1578,7 @@ Status run_blind_psf(Context& ctx, const float* img, Dims id, const float* ker, 
   cudaStream_t st = ctx.exec_stream();
   const VolPlan& P = pe->P;
   const long long n = wd.n();
-  if (ws->accel_cap < n) {
-    for (float*& b : ws->accel) {
-      cudaFree(b);
-      b = nullptr;
-    }
-    ws->accel_cap = 0;
-    for (float*& b : ws->accel) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
-    ws->accel_cap = n;
-  }
+  CL_TRY(ensure_volumes(ws->accel, &ws->accel_cap, n));
   if (!ws->HG) CL_CHECK(dev_alloc((void**)&ws->HG, sizeof(float2) * (size_t)ws->spec_cap));
   float* o = ws->accel[0];
   float* h = ws->accel[1];
