@@ -200,3 +200,12 @@ def test_emulated_idiv_restoration_matches_oracle(emu, tmp_path, oracle_lib, cas
         ref64 = oracle_lib.idiv_cg(img, psf, iters, alpha, precision="f64")
         ref32 = oracle_lib.idiv_cg(img, psf, iters, alpha)
         assert rel_l2(got, ref64) <= max(2e-6, 4 * rel_l2(ref32, ref64))
+
+
+def test_emulated_idiv_restoration_zero_iterations_returns_the_image(emu, tmp_path):
+    # no step taken: s = (sqrt g)^2 on the image region, non-negative
+    d = load_golden("small_even")
+    img = d["image"]
+    out = run_emu(emu, tmp_path, "idiv", img, d["psf"], 0)
+    assert out.min() >= 0
+    assert rel_l2(out, np.maximum(img, 0)) <= 1e-6
