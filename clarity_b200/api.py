@@ -51,8 +51,10 @@ PUBLIC_SYMBOLS = [
 ]
 EXTENSION_SYMBOLS = [
     "clarityx_last_error", "clarityx_set_device", "clarityx_inject_device_alloc_failure",
-    "clarityx_trim", "clarityx_synchronize", "clarityx_convolve_device",
-    "clarityx_wiener_device", "clarityx_ml_device", "clarityx_blind_ml_device",
+    "clarityx_trim", "clarityx_synchronize", "clarityx_inject_wait_timeout",
+    "clarityx_convolve_device",
+    "clarityx_wiener_device", "clarityx_ml_device", "clarityx_correlate_device",
+    "clarityx_ml_correlate_device", "clarityx_blind_ml_device",
     "clarityx_jvc_device", "clarityx_idivergence", "clarityx_plan_info",
     "clarityx_launch_count", "clarityx_timing_enable", "clarityx_timing_collect",
     "clarityx_convolve_noalloc", "clarityx_ml_batch_device", "clarityx_autotune",
@@ -63,6 +65,7 @@ EXTENSION_SYMBOLS = [
     "clarityx_nn_conv_in_wgrad", "clarityx_nn_head", "clarityx_nn_head_loss_grad",
     "clarityx_nn_pool2", "clarityx_nn_merge_skip_grad", "clarityx_nn_up_grad",
     "clarityx_nn_adam", "clarityx_nn_pack_weights",
+    "clarityx_ml_learned_device", "clarityx_nn_predict", "clarityx_nn_param_count",
 ]
 BATCH_GRAPH = 1  # CLARITYX_BATCH_GRAPH
 
@@ -130,7 +133,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_trim.restype = i
         L.clarityx_synchronize.argtypes = [vp]
         L.clarityx_synchronize.restype = i
+        L.clarityx_inject_wait_timeout.argtypes = [vp]
+        L.clarityx_inject_wait_timeout.restype = i
         for name, extra in [("clarityx_convolve_device", []),
+                            ("clarityx_correlate_device", []),
+                            ("clarityx_ml_correlate_device", [i]),
                             ("clarityx_wiener_device", [f]),
                             ("clarityx_ml_device", [i]),
                             ("clarityx_blind_ml_device", [i]),
@@ -160,6 +167,12 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_blind_ml_psf_device.restype = i
         L.clarityx_idiv_deconvolve_device.argtypes = [vp, Dim3, vp, Dim3, vp, i, C.c_float, vp]
         L.clarityx_idiv_deconvolve_device.restype = i
+        L.clarityx_ml_learned_device.argtypes = [vp, Dim3, vp, Dim3, vp, C.c_longlong, i, vp, i,
+                                                 vp, vp]
+        L.clarityx_ml_learned_device.restype = i
+        L.clarityx_nn_predict.argtypes = [vp, C.c_longlong, vp, Dim3, vp, vp]
+        L.clarityx_nn_predict.restype = i
+        L.clarityx_nn_param_count.restype = C.c_longlong
         L.clarityx_autotune.argtypes = [i]
         L.clarityx_autotune.restype = None
         L.clarityx_launch_count.restype = C.c_longlong
@@ -218,6 +231,20 @@ def inject_device_alloc_failure(countdown: int) -> None:
 
 def trim() -> None:
     _check(load().clarityx_trim())
+
+
+def synchronize(stream=None) -> None:
+    """clarityx_synchronize: wait for `stream` (None: every stream of the
+    library's device) and raise the first asynchronous failure, such as a
+    device-side bounded wait that gave up."""
+    ptr = None if stream is None else C.c_void_p(stream.cuda_stream)
+    _check(load().clarityx_synchronize(ptr))
+
+
+def inject_wait_timeout(stream=None) -> None:
+    """clarityx_inject_wait_timeout: enqueue a kernel whose bounded wait runs
+    out (no copy in flight), recording a timeout as a fused pass would."""
+    _check(load().clarityx_inject_wait_timeout(_stream_ptr(stream)))
 
 
 # ------------------------------------------------------------- utilities
@@ -355,6 +382,19 @@ def convolve_device(image, kernel, out, stream=None):
     return _dev("clarityx_convolve_device", image, kernel, out, [], stream)
 
 
+def correlate_device(image, kernel, out, stream=None):
+    """clarityx_correlate_device: circular correlation with the kernel (its
+    spectrum conjugated in the z pass; an opt-in with no reference
+    counterpart)."""
+    return _dev("clarityx_correlate_device", image, kernel, out, [], stream)
+
+
+def ml_correlate_device(image, kernel, out, iterations, stream=None):
+    """clarityx_ml_correlate_device: RL whose second convolution per
+    iteration is a correlation with the kernel (conjugated OTF)."""
+    return _dev("clarityx_ml_correlate_device", image, kernel, out, [int(iterations)], stream)
+
+
 def convolve_noalloc(image, kernel, out, stream=None):
     """clarityx_convolve_noalloc: convolution of device tensors with all
     scratch in the library's fixed 32 MiB device array (no allocation)."""
@@ -445,6 +485,42 @@ def ml_accel_device(image, kernel, out, iterations, idiv=None, stream=None, star
         vp(out.data_ptr()), int(iterations), vp(idiv.data_ptr()) if idiv is not None else None,
         _stream_ptr(stream)))
     return out
+
+
+def ml_learned_device(image, kernel, params, out, pre, post, idiv=None, stream=None):
+    """clarityx_ml_learned_device: RL `pre` iterations, the learned-start
+    network's prediction (FP32 parameter tensor `params` on the device), RL
+    resumed for `post` iterations (optional float64 trace of post + 1
+    entries)."""
+    for t in (image, kernel, out, params):
+        if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+            raise ValueError("device variants need contiguous float32 CUDA tensors")
+    if idiv is not None and not (idiv.is_cuda and str(idiv.dtype) == "torch.float64"
+                                 and idiv.numel() >= max(int(post), 0) + 1):
+        raise ValueError("idiv must be a float64 CUDA tensor of `post` + 1 entries")
+    vp = C.c_void_p
+    _check(load().clarityx_ml_learned_device(
+        vp(image.data_ptr()), dim3(image), vp(kernel.data_ptr()), dim3(kernel),
+        vp(params.data_ptr()), params.numel(), int(pre), vp(out.data_ptr()), int(post),
+        vp(idiv.data_ptr()) if idiv is not None else None, _stream_ptr(stream)))
+    return out
+
+
+def nn_predict(params, x, out, stream=None):
+    """clarityx_nn_predict: the learned-start network's advanced estimate
+    from the volume x (domain transforms fused into its first and last
+    kernels)."""
+    for t in (params, x, out):
+        if not (t.is_cuda and t.is_contiguous() and str(t.dtype) == "torch.float32"):
+            raise ValueError("nn_predict needs contiguous float32 CUDA tensors")
+    vp = C.c_void_p
+    _check(load().clarityx_nn_predict(vp(params.data_ptr()), params.numel(), vp(x.data_ptr()),
+                                      dim3(x), vp(out.data_ptr()), _stream_ptr(stream)))
+    return out
+
+
+def nn_param_count() -> int:
+    return int(load().clarityx_nn_param_count())
 
 
 def maximum_likelihood_deconvolve_u16(image, kernel, iterations: int) -> np.ndarray:

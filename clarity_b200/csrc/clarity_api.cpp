@@ -43,6 +43,102 @@ struct Staging {
   size_t img_cap = 0, ker_cap = 0, out_cap = 0;
 } g_stage;
 
+// Library-owned pinned bounce buffers for callers whose host buffers are
+// pageable (every reference caller allocates with malloc or new,
+// src/Memory.cxx:97-156 copies from them synchronously).  A copy is cut
+// into chunks that alternate between two pinned buffers: the host copies
+// chunk k into one while the DMA engine moves chunk k-1 out of the other.
+// Buffers the caller pinned itself (cudaHostAlloc, cudaHostRegister) are
+// copied directly.
+struct PinnedBounce {
+  static constexpr size_t kChunk = size_t(8) << 20;
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+} g_bounce;
+
+bool host_is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // an unregistered pointer is not an error here
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+cudaError_t bounce_ready() {
+  for (int i = 0; i < 2; ++i) {
+    if (!g_bounce.buf[i]) {
+      cudaError_t e = cudaHostAlloc(&g_bounce.buf[i], PinnedBounce::kChunk, cudaHostAllocPortable);
+      if (e != cudaSuccess) return e;
+    }
+    if (!g_bounce.ev[i]) {
+      cudaError_t e = cudaEventCreateWithFlags(&g_bounce.ev[i], cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+void free_bounce() {
+  for (int i = 0; i < 2; ++i) {
+    if (g_bounce.buf[i]) cudaFreeHost(g_bounce.buf[i]);
+    if (g_bounce.ev[i]) cudaEventDestroy(g_bounce.ev[i]);
+  }
+  g_bounce = PinnedBounce();
+}
+
+// host -> device on `st`, asynchronous for pinned sources; a pageable source
+// has been read completely when this returns.
+cudaError_t upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return cudaSuccess;
+  if (host_is_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  cudaError_t e = bounce_ready();
+  if (e != cudaSuccess) return e;
+  const char* s = static_cast<const char*>(src);
+  char* d = static_cast<char*>(dst);
+  for (size_t off = 0, k = 0; off < bytes; off += PinnedBounce::kChunk, ++k) {
+    const int i = (int)(k & 1);
+    const size_t n = std::min(PinnedBounce::kChunk, bytes - off);
+    if ((e = cudaEventSynchronize(g_bounce.ev[i])) != cudaSuccess) return e;  // buffer free
+    std::memcpy(g_bounce.buf[i], s + off, n);
+    if ((e = cudaMemcpyAsync(d + off, g_bounce.buf[i], n, cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess)
+      return e;
+    if ((e = cudaEventRecord(g_bounce.ev[i], st)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// device -> host on `st`; complete (the host buffer written) when it returns
+// for a pageable destination, asynchronous for a pinned one.
+cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return cudaSuccess;
+  if (host_is_pinned(dst)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = bounce_ready();
+  if (e != cudaSuccess) return e;
+  const char* s = static_cast<const char*>(src);
+  char* d = static_cast<char*>(dst);
+  const size_t nch = (bytes + PinnedBounce::kChunk - 1) / PinnedBounce::kChunk;
+  auto issue = [&](size_t k) -> cudaError_t {
+    const int i = (int)(k & 1);
+    const size_t off = k * PinnedBounce::kChunk, n = std::min(PinnedBounce::kChunk, bytes - off);
+    cudaError_t r = cudaEventSynchronize(g_bounce.ev[i]);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(g_bounce.buf[i], s + off, n,
+                                              cudaMemcpyDeviceToHost, st);
+    if (r == cudaSuccess) r = cudaEventRecord(g_bounce.ev[i], st);
+    return r;
+  };
+  if ((e = issue(0)) != cudaSuccess) return e;
+  for (size_t k = 0; k < nch; ++k) {
+    if (k + 1 < nch && (e = issue(k + 1)) != cudaSuccess) return e;
+    const int i = (int)(k & 1);
+    const size_t off = k * PinnedBounce::kChunk, n = std::min(PinnedBounce::kChunk, bytes - off);
+    if ((e = cudaEventSynchronize(g_bounce.ev[i])) != cudaSuccess) return e;
+    std::memcpy(d + off, g_bounce.buf[i], n);
+  }
+  return cudaSuccess;
+}
+
 void set_error(const char* msg) {
   std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg ? msg : "");
 }
@@ -80,6 +176,7 @@ void free_staging() {
   cudaFree(g_stage.ker);
   cudaFree(g_stage.out);
   g_stage = Staging();
+  free_bounce();
 }
 
 // Common path of the host-buffer algorithms: validate, upload, run, download.
@@ -98,21 +195,22 @@ ClarityResult_t host_call(const float* in, Clarity_Dim3 id, const float* ker,
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   ctx->clear_stream();
+  // a failure recorded by earlier asynchronous work is reported, not hidden
+  // behind this call's success
+  Status s = ctx->check_device_errors();
+  if (!s.ok()) return report(s);
   const size_t ni = (size_t)nvox(id), nk = (size_t)nvox(kd);
-  Status s = grow(&g_stage.img, &g_stage.img_cap, ni);
+  s = grow(&g_stage.img, &g_stage.img_cap, ni);
   if (s.ok()) s = grow(&g_stage.ker, &g_stage.ker_cap, nk);
   if (s.ok()) s = grow(&g_stage.out, &g_stage.out_cap, ni);
   if (!s.ok()) return report(s);
   cudaStream_t st = ctx->exec_stream();
-  cudaError_t e = cudaMemcpyAsync(g_stage.img, in, sizeof(float) * ni,
-                                  cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(g_stage.ker, ker, sizeof(float) * nk,
-                        cudaMemcpyHostToDevice, st);
+  cudaError_t e = upload(g_stage.img, in, sizeof(float) * ni, st);
+  if (e == cudaSuccess) e = upload(g_stage.ker, ker, sizeof(float) * nk, st);
   if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "host to device copy"));
   s = run(*ctx, g_stage.img, to_dims(id), g_stage.ker, to_dims(kd), g_stage.out);
   if (!s.ok()) return report(s);
-  e = cudaMemcpyAsync(out, g_stage.out, sizeof(float) * ni, cudaMemcpyDeviceToHost, st);
+  e = download(out, g_stage.out, sizeof(float) * ni, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "device to host copy"));
   return report(ctx->check_device_errors());
@@ -132,8 +230,12 @@ ClarityResult_t device_call(const float* in, Clarity_Dim3 id, const float* ker,
   if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
+  // a bounded wait of earlier work that gave up is reported here (that
+  // work's result is not valid) and nothing is enqueued
+  Status s = ctx->check_device_errors();
+  if (!s.ok()) return report(s);
   ctx->set_stream(static_cast<cudaStream_t>(stream));
-  Status s = run(*ctx, in, to_dims(id), ker, to_dims(kd), out);
+  s = run(*ctx, in, to_dims(id), ker, to_dims(kd), out);
   ctx->clear_stream();
   return report(s);
 }
@@ -173,6 +275,12 @@ ClarityResult_t Clarity_Register(void) {
       return fail(CLARITY_INVALID_OPERATION,
                   std::string("device is not sm_100 class: ") + prop.name);
     g_ctx = new Context(g_device);
+    const Status is = g_ctx->init();
+    if (!is.ok()) {
+      delete g_ctx;
+      g_ctx = nullptr;
+      return report(is);
+    }
     g_ctx->set_autotune(g_autotune);
     if (std::getenv("CLARITY_LOG"))
       std::fprintf(stderr, "clarity: device %d '%s', %zu MB\n", g_device, prop.name,
@@ -372,13 +480,33 @@ ClarityResult_t clarityx_trim(void) {
 }
 
 ClarityResult_t clarityx_synchronize(void* stream) {
-  Context* ctx = g_ctx;
+  Context* ctx;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx = g_ctx;
+  }
   if (!ctx) return fail(CLARITY_INVALID_OPERATION, "not registered");
   cudaSetDevice(ctx->device());
-  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream();
-  cudaError_t e = cudaStreamSynchronize(st);
+  // NULL: every stream of the device (the library's own included)
+  const cudaError_t e = stream ? cudaStreamSynchronize(static_cast<cudaStream_t>(stream))
+                               : cudaDeviceSynchronize();
   if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "synchronize"));
-  return CLARITY_SUCCESS;
+  return report(ctx->check_device_errors());
+}
+
+ClarityResult_t clarityx_inject_wait_timeout(void* stream) {
+  Context* ctx;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx = g_ctx;
+  }
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "not registered");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device());
+  ctx->set_stream(static_cast<cudaStream_t>(stream));
+  const Status s = clarity::inject_wait_timeout(*ctx);
+  ctx->clear_stream();
+  return report(s);
 }
 
 ClarityResult_t clarityx_convolve_device(const float* image, Clarity_Dim3 imageDim,
@@ -407,6 +535,65 @@ ClarityResult_t clarityx_ml_device(const float* image, Clarity_Dim3 imageDim,
                          float* o) {
                        return clarity::run_rl(c, i, id, k, kd, o, iterations);
                      });
+}
+
+ClarityResult_t clarityx_correlate_device(const float* image, Clarity_Dim3 imageDim,
+                                          const float* kernel, Clarity_Dim3 kernelDim,
+                                          float* out, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) { return clarity::run_correlate(c, i, id, k, kd, o); });
+}
+
+ClarityResult_t clarityx_ml_correlate_device(const float* image, Clarity_Dim3 imageDim,
+                                             const float* kernel, Clarity_Dim3 kernelDim,
+                                             float* out, int iterations, void* stream) {
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_rl_correlate(c, i, id, k, kd, o, iterations);
+                     });
+}
+
+ClarityResult_t clarityx_ml_learned_device(const float* image, Clarity_Dim3 imageDim,
+                                           const float* kernel, Clarity_Dim3 kernelDim,
+                                           const float* params, long long nparams, int pre,
+                                           float* out, int post, double* idiv, void* stream) {
+  if (!params) return fail(CLARITY_INVALID_ARGUMENT, "NULL network parameters");
+  if (nparams != clarity::nn_param_count())
+    return fail(CLARITY_INVALID_ARGUMENT,
+                "network parameters: expected " + std::to_string(clarity::nn_param_count()) +
+                    " floats, got " + std::to_string(nparams));
+  return device_call(image, imageDim, kernel, kernelDim, out, stream,
+                     [&](Context& c, const float* i, Dims id, const float* k, Dims kd,
+                         float* o) {
+                       return clarity::run_ml_learned(c, i, id, k, kd, params, pre, o, post,
+                                                      idiv);
+                     });
+}
+
+long long clarityx_nn_param_count(void) { return clarity::nn_param_count(); }
+
+ClarityResult_t clarityx_nn_predict(const float* params, long long nparams, const float* x,
+                                    Clarity_Dim3 dim, float* out, void* stream) {
+  if (!params || !x || !out) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
+  if (!dims_ok(dim)) return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
+  if (nparams != clarity::nn_param_count())
+    return fail(CLARITY_INVALID_ARGUMENT, "network parameters: wrong count");
+  Context* ctx;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ctx = g_ctx;
+  }
+  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device());
+  Status s = ctx->check_device_errors();
+  if (!s.ok()) return report(s);
+  ctx->set_stream(static_cast<cudaStream_t>(stream));
+  s = clarity::nn_predict(*ctx, params, x, dim.z, dim.y, dim.x, out);
+  ctx->clear_stream();
+  return report(s);
 }
 
 ClarityResult_t clarityx_idiv_deconvolve_device(const float* image, Clarity_Dim3 imageDim,
@@ -450,21 +637,23 @@ ClarityResult_t clarityx_ml_u16(const uint16_t* image, Clarity_Dim3 imageDim,
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   ctx->clear_stream();
+  Status s = ctx->check_device_errors();
+  if (!s.ok()) return report(s);
   const size_t ni = (size_t)nvox(imageDim), nk = (size_t)nvox(kernelDim);
   // uint16 data lands in the output staging buffer (sized for either
   // volume), is cast into the image / kernel staging buffers, and the result
   // is cast back into the image staging buffer
-  Status s = grow(&g_stage.img, &g_stage.img_cap, ni);
+  s = grow(&g_stage.img, &g_stage.img_cap, ni);
   if (s.ok()) s = grow(&g_stage.ker, &g_stage.ker_cap, nk);
   if (s.ok()) s = grow(&g_stage.out, &g_stage.out_cap, std::max(ni, nk));
   if (!s.ok()) return report(s);
   cudaStream_t st = ctx->exec_stream();
   uint16_t* raw = reinterpret_cast<uint16_t*>(g_stage.out);
-  cudaError_t e = cudaMemcpyAsync(raw, image, sizeof(uint16_t) * ni, cudaMemcpyHostToDevice, st);
+  cudaError_t e = upload(raw, image, sizeof(uint16_t) * ni, st);
   if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "host to device copy"));
   s = clarity::cast_u16_to_f32(*ctx, raw, g_stage.img, (long long)ni);
   if (!s.ok()) return report(s);
-  e = cudaMemcpyAsync(raw, kernel, sizeof(uint16_t) * nk, cudaMemcpyHostToDevice, st);
+  e = upload(raw, kernel, sizeof(uint16_t) * nk, st);
   if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "host to device copy"));
   s = clarity::cast_u16_to_f32(*ctx, raw, g_stage.ker, (long long)nk);
   if (s.ok())
@@ -474,7 +663,7 @@ ClarityResult_t clarityx_ml_u16(const uint16_t* image, Clarity_Dim3 imageDim,
   uint16_t* res = reinterpret_cast<uint16_t*>(g_stage.img);
   s = clarity::cast_f32_to_u16(*ctx, g_stage.out, res, (long long)ni);
   if (!s.ok()) return report(s);
-  e = cudaMemcpyAsync(out, res, sizeof(uint16_t) * ni, cudaMemcpyDeviceToHost, st);
+  e = download(out, res, sizeof(uint16_t) * ni, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return report(clarity::status_from_cuda(e, "device to host copy"));
   return report(ctx->check_device_errors());
@@ -526,9 +715,11 @@ ClarityResult_t clarityx_ml_batch_device(int count, const float* const* images,
   if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
+  Status s = ctx->check_device_errors();
+  if (!s.ok()) return report(s);
   ctx->set_stream(static_cast<cudaStream_t>(stream));
-  Status s = clarity::run_rl_batch(*ctx, count, images, ids.data(), kernels, kds.data(), outs,
-                                   iterations, (flags & CLARITYX_BATCH_GRAPH) != 0);
+  s = clarity::run_rl_batch(*ctx, count, images, ids.data(), kernels, kds.data(), outs,
+                            iterations, (flags & CLARITYX_BATCH_GRAPH) != 0);
   ctx->clear_stream();
   return report(s);
 }

@@ -340,6 +340,17 @@ __global__ void k_copy(const float* __restrict__ a, float* __restrict__ b,
 
 static constexpr int kReduceBlocks = 592;  // 4 x 148 SMs
 
+// hc = conj(h) over a spectrum: the OTF of the reflected kernel h(-x), whose
+// product is a correlation with h.
+__global__ void k_conj_spectrum(const float2* __restrict__ h, float2* __restrict__ hc,
+                                long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float2 v = h[i];
+    hc[i] = make_float2(v.x, -v.y);
+  }
+}
+
 // uint16 raw volumes (the reference's DeconvolveRawImages app,
 // apps/DeconvolveRawImages/DeconvolveRawImages.cxx:91-116): cast in, and cast
 // out as x86 does for static_cast<unsigned short>(float) -- truncation to a
@@ -420,9 +431,19 @@ __global__ void k_idiv(const float* __restrict__ g, const float* __restrict__ gh
 
 
 // --------------------------------------------------------------- context
-Context::Context(int device) : device_(device) {
-  cudaSetDevice(device);
-  cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+Context::Context(int device) : device_(device) {}
+
+Status Context::init() {
+  CL_CHECK(cudaSetDevice(device_));
+  CL_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  void* h = nullptr;
+  CL_CHECK(cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable));
+  err_host_ = static_cast<int*>(h);
+  *reinterpret_cast<volatile int*>(err_host_) = 0;
+  void* d = nullptr;
+  CL_CHECK(cudaHostGetDevicePointer(&d, h, 0));
+  err_dev_ = static_cast<int*>(d);
+  return Status::Ok();
 }
 
 Context::~Context() {
@@ -433,10 +454,10 @@ Context::~Context() {
   for (auto& kv : plans_) {
     cudaFree(kv.second->tw);
     cudaFree(kv.second->xrev);
-    cudaFree(kv.second->err);
   }
   plans_.clear();
   if (stream_) cudaStreamDestroy(stream_);
+  if (err_host_) cudaFreeHost(err_host_);
 }
 
 static void free_workspace(Workspace& w) {
@@ -455,6 +476,21 @@ void Context::release_workspaces() {
   free_workspace(ws_);
   for (auto& w : slots_) free_workspace(*w);
   slots_.clear();
+  cudaFree(aux_);
+  aux_ = nullptr;
+  aux_cap_ = 0;
+}
+
+Status Context::aux_scratch(size_t bytes, void** out) {
+  if (aux_cap_ < bytes || !aux_) {
+    cudaFree(aux_);
+    aux_ = nullptr;
+    aux_cap_ = 0;
+    CL_CHECK(dev_alloc(&aux_, bytes));
+    aux_cap_ = bytes;
+  }
+  *out = aux_;
+  return Status::Ok();
 }
 
 Status Context::batch_stream(int i, cudaStream_t* out) {
@@ -488,8 +524,7 @@ Status Context::build_entry(const VolPlan& P0, std::unique_ptr<PlanEntry>* out) 
   const VolPlan& P = pe->P;
   CL_CHECK(dev_alloc((void**)&pe->tw, sizeof(float2) * P.twiddle_count));
   CL_CHECK(dev_alloc((void**)&pe->xrev, sizeof(int) * std::max(P.xrev_count, 1)));
-  CL_CHECK(dev_alloc((void**)&pe->err, sizeof(int)));
-  CL_CHECK(cudaMemsetAsync(pe->err, 0, sizeof(int), exec_stream()));
+  pe->err = err_dev_;
   std::vector<int> rev;
   std::vector<TwTable> tabs;
   plan_tables(P, &rev, &tabs);
@@ -511,7 +546,6 @@ Status Context::build_entry(const VolPlan& P0, std::unique_ptr<PlanEntry>* out) 
 static void free_entry(PlanEntry& pe) {
   cudaFree(pe.tw);
   cudaFree(pe.xrev);
-  cudaFree(pe.err);
 }
 
 Status Context::plan(const Dims& wd, const PlanEntry** out) {
@@ -542,17 +576,35 @@ Status Context::plan(const Dims& wd, const PlanEntry** out) {
 }
 
 Status Context::check_device_errors() {
-  for (auto& kv : plans_) {
-    int e = 0;
-    CL_CHECK(cudaMemcpy(&e, kv.second->err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e != 0) {
-      CL_CHECK(cudaMemset(kv.second->err, 0, sizeof(int)));
-      Status s;
-      s.code = CLARITY_INVALID_OPERATION;
-      s.msg = "a device-side wait timed out (code " + std::to_string(e) + ")";
-      return s;
-    }
-  }
+  if (!err_host_) return Status::Ok();
+  const int e = __atomic_exchange_n(err_host_, 0, __ATOMIC_ACQ_REL);
+  if (e == 0) return Status::Ok();
+  Status s;
+  s.code = CLARITY_INVALID_OPERATION;
+  s.msg = e == kErrWaitTimeout
+              ? "a device-side wait timed out; the result of the call that ran it is not valid"
+              : "a device-side copy address was misaligned (code " + std::to_string(e) +
+                    "); the result of the call that ran it is not valid";
+  return s;
+}
+
+// Failure-detection self test: one thread arms an mbarrier for 16 bytes that
+// no copy will ever deliver and waits on it with a bound of `limit` polls,
+// exactly as a fused pass waits for its tile.  The wait gives up and records
+// kErrWaitTimeout in the error word.  No copy is issued, so nothing is left
+// in flight when the block exits.
+__global__ void k_wait_timeout_probe(int* err, long long limit) {
+  __shared__ alignas(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  mbar_arrive_expect_tx(&bar, 16);
+  mbar_wait_bounded(&bar, 0, err, limit);
+}
+
+Status inject_wait_timeout(Context& ctx) {
+  count_small();
+  CLARITY_LAUNCH(k_wait_timeout_probe, 1, 32, 0, ctx.exec_stream())(ctx.err_dev(), 1ll << 14);
+  CL_CHECK(cudaGetLastError());
   return Status::Ok();
 }
 
@@ -795,6 +847,29 @@ Status run_convolve(Context& ctx, const float* img, Dims id, const float* ker,
   return Status::Ok();
 }
 
+// Circular correlation: Clarity_Convolve's passes with the conjugated OTF
+// applied in the z pass.
+Status run_correlate(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                     float* out) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  const VolPlan& P = pe->P;
+  CL_TRY(make_otf(ctx, *pe, ker, kd, wd, ws->H, nullptr));
+  if (!ws->HG) CL_CHECK(dev_alloc((void**)&ws->HG, sizeof(float2) * (size_t)ws->spec_cap));
+  count_small();
+  CLARITY_LAUNCH(k_conj_spectrum, kReduceBlocks, 256, 0, ctx.exec_stream())(ws->H, ws->HG,
+                                                                            P.spec_elems);
+  CL_CHECK(cudaGetLastError());
+  ProImage pro{image_src(img, id), P.xmode};
+  CL_TRY(xy_forward(ctx, *pe, pro, ws->S));
+  CL_TRY(z_pass(ctx, *pe, ModOTF{ws->HG, inv_volume(wd)}, ws->S, ws->S));
+  EpiClip epi{out, id.x, id.y, id.z, nullptr, P.xmode};
+  CL_TRY(xy_inverse(ctx, *pe, epi, ws->S));
+  return Status::Ok();
+}
+
 Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
                   Dims kd, float* out, float eps) {
   const PlanEntry* pe;
@@ -833,6 +908,7 @@ Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
 // the image's energy.
 struct RLRoles {
   const float2* otf = nullptr;  // fully transformed OTF (nullptr: ws.H)
+  const float2* otf2 = nullptr; // the second convolution's OTF (nullptr: otf)
   Dims start_dims{0, 0, 0};     // start's extent on the work box (0: the image's)
   bool unit_energy = false;     // rescale to sum 1 instead of sum(image)
 };
@@ -887,6 +963,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
   const Dims sd = roles.start_dims.x > 0 ? roles.start_dims : id;
   const ImageSrc u0 = start ? image_src(start, sd) : g;
   const float2* H = roles.otf ? roles.otf : ws.H;
+  const float2* H2 = roles.otf2 ? roles.otf2 : H;
   const WorkVol wv{wd.x, wd.y, wd.z};
   const float scale_n = inv_volume(wd);
   float* sdev = ws.fscal;  // deferred flux scale
@@ -921,7 +998,7 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
     }
     // the ratio is zero in planes z >= Z (the image is zero there): P3 does
     // not write them and this pass reads them as zeros
-    ModOTF m4{H, scale_n};
+    ModOTF m4{H2, scale_n};
     m4.zn = id.z;
     CL_TRY(z_pass(ctx, pe, m4, ws.S, ws.S));
     EpiRLProduct epi;
@@ -964,11 +1041,25 @@ static Status rl_core(Context& ctx, const PlanEntry& pe, Workspace& ws,
   return Status::Ok();
 }
 
+// The conjugated OTF (ws.HG) from ws.H, for the correlation opt-ins.
+static Status conj_otf(Context& ctx, const PlanEntry& pe, Workspace& ws) {
+  if (!ws.HG) CL_CHECK(dev_alloc((void**)&ws.HG, sizeof(float2) * (size_t)ws.spec_cap));
+  count_small();
+  CLARITY_LAUNCH(k_conj_spectrum, kReduceBlocks, 256, 0, ctx.exec_stream())(ws.H, ws.HG,
+                                                                            pe.P.spec_elems);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
 // One Richardson-Lucy solve on prepared plan and workspace, enqueued on
-// ctx.exec_stream(): OTF, the iterations, the clipped result.
+// ctx.exec_stream(): OTF, the iterations, the clipped result.  correlate:
+// the second convolution of each iteration uses the conjugated OTF (a
+// correlation with the kernel; the reference convolves twice,
+// src/MaximumLikelihoodDeconvolve.cxx:57,65).
 static Status rl_solve(Context& ctx, const PlanEntry& pe, Workspace& ws, const float* img,
                        Dims id, const float* ker, Dims kd, Dims wd, float* out, int iters,
-                       const float* start = nullptr, double* idiv = nullptr) {
+                       const float* start = nullptr, double* idiv = nullptr,
+                       bool correlate = false) {
   cudaStream_t st = ctx.exec_stream();
   if (iters <= 0) {
     // the reference leaves the output unwritten; return the input image
@@ -978,7 +1069,12 @@ static Status rl_solve(Context& ctx, const PlanEntry& pe, Workspace& ws, const f
     return Status::Ok();
   }
   CL_TRY(make_otf(ctx, pe, ker, kd, wd, ws.H, nullptr));
-  CL_TRY(rl_core(ctx, pe, ws, img, id, wd, iters, true, start, idiv));
+  RLRoles roles;
+  if (correlate) {
+    CL_TRY(conj_otf(ctx, pe, ws));
+    roles.otf2 = ws.HG;
+  }
+  CL_TRY(rl_core(ctx, pe, ws, img, id, wd, iters, true, start, idiv, roles));
   count_small();
   CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, st)(ws.u, wd.x, wd.y, out, id.x, id.y, id.z,
                                                     ws.fscal);
@@ -1008,6 +1104,15 @@ Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
   Dims wd;
   CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
   return rl_solve(ctx, *pe, *ws, img, id, ker, kd, wd, out, iters);
+}
+
+Status run_rl_correlate(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                        float* out, int iters) {
+  const PlanEntry* pe;
+  Workspace* ws;
+  Dims wd;
+  CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
+  return rl_solve(ctx, *pe, *ws, img, id, ker, kd, wd, out, iters, nullptr, nullptr, true);
 }
 
 Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
@@ -1468,15 +1573,6 @@ static Status conv_work(Context& ctx, const PlanEntry& pe, Workspace& ws, const 
   CL_TRY(z_pass(ctx, pe, ModOTF{otf, inv_volume(wd)}, ws.S, ws.S));
   CL_TRY(xy_inverse(ctx, pe, EpiWork{v, wv, P.xmode}, ws.S));
   return Status::Ok();
-}
-
-__global__ void k_conj_spectrum(const float2* __restrict__ h, float2* __restrict__ hc,
-                                long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const float2 v = h[i];
-    hc[i] = make_float2(v.x, -v.y);
-  }
 }
 
 Status run_idiv_cg(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,

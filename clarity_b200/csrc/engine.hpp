@@ -38,7 +38,7 @@ struct PlanEntry {
   VolPlan P;
   float2* tw = nullptr;  // twiddle tables (FP64-generated, rounded)
   int* xrev = nullptr;   // natural x frequency -> smem slot after x passes
-  int* err = nullptr;    // device error word: nonzero after a bounded wait gave up
+  int* err = nullptr;    // the context's error word (device alias; not owned)
 };
 
 
@@ -71,7 +71,13 @@ class Context {
  public:
   explicit Context(int device);
   ~Context();
+  // Creates the stream and the error word; call once after construction.
+  Status init();
   int device() const { return device_; }
+  // Error word the kernels write when a bounded wait gives up or a copy
+  // address is misaligned: one int of mapped pinned host memory, so the host
+  // reads it without a device synchronisation.  Device alias for kernels.
+  int* err_dev() const { return err_dev_; }
   cudaStream_t stream() const { return stream_; }
   // The stream work is enqueued on: the caller's (any handle, 0 included,
   // which is the legacy default stream) while one is set, else the context's
@@ -99,7 +105,11 @@ class Context {
   void set_autotune(bool on) { autotune_ = on; }
   bool autotune() const { return autotune_; }
   void release_workspaces();
-  // Reads and clears every plan's device error word (synchronous).
+  // One growable device block for auxiliary scratch (the learned-start
+  // network's weights and activations); freed by release_workspaces.
+  Status aux_scratch(size_t bytes, void** out);
+  // Reads and clears the error word (no synchronisation: it reports what
+  // kernels that have finished recorded).
   Status check_device_errors();
 
   std::mutex mu;  // serialises API calls on this context
@@ -107,6 +117,10 @@ class Context {
  private:
   int device_;
   cudaStream_t stream_ = nullptr;
+  int* err_host_ = nullptr;  // mapped pinned host memory
+  int* err_dev_ = nullptr;
+  void* aux_ = nullptr;
+  size_t aux_cap_ = 0;
   cudaStream_t user_stream_ = nullptr;
   bool has_user_stream_ = false;
   Status build_entry(const VolPlan& P, std::unique_ptr<PlanEntry>* out);
@@ -130,6 +144,13 @@ Status run_convolve(Context& ctx, const float* img, Dims id, const float* ker,
                     Dims kd, float* out);
 Status run_wiener(Context& ctx, const float* img, Dims id, const float* ker,
                   Dims kd, float* out, float eps);
+// Circular correlation with the kernel (the conjugated OTF in the z pass).
+Status run_correlate(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                     float* out);
+// Richardson-Lucy whose second convolution per iteration is a correlation
+// with the kernel (conjugated OTF).
+Status run_rl_correlate(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                        float* out, int iters);
 Status run_rl(Context& ctx, const float* img, Dims id, const float* ker,
               Dims kd, float* out, int iters);
 // Richardson-Lucy from a given first estimate (image-sized, nullptr: the
@@ -165,6 +186,21 @@ Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
 Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
                Dims kd, float* out, int iters, float image_max,
                const float* smooth_sigma, int smooth_interval);
+// Learned start (nn.cu): RL `pre` iterations, the 3-D U-Net's prediction from
+// that iterate (FP32 parameter vector `params` of nn_param_count() floats, on
+// the device), RL resumed from the prediction for `post` iterations; idiv as
+// run_rl_ex for the resumed part.  Image dimensions must be multiples of 8.
+long long nn_param_count();
+Status run_ml_learned(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                      const float* params, int pre, float* out, int post, double* idiv);
+// The network's prediction alone: out = max(0, m ((x/m + 0.01) e^r - 0.01)),
+// r = U-Net(log(x/m + 0.01)), m = mean(x); x and out are D x H x W volumes.
+Status nn_predict(Context& ctx, const float* params, const float* x, int D, int H, int W,
+                  float* out);
+// Failure-detection self test: enqueues a one-thread kernel whose bounded
+// mbarrier wait runs out (no copy is issued) and records a timeout in the
+// context's error word, as a fused pass would.
+Status inject_wait_timeout(Context& ctx);
 // FP64 I-divergence of g against ghat (both unpadded device volumes).
 Status run_idivergence(Context& ctx, const float* g, const float* ghat,
                        long long n, double* result);

@@ -26,6 +26,7 @@
 
 #include "engine.hpp"
 #include "launch_macro.cuh"
+#include "ops.cuh"
 
 namespace clarity {
 namespace nn {
@@ -818,3 +819,273 @@ CLARITY_API ClarityResult_t clarityx_nn_pack_weights(const float* w, int cout, i
 }
 
 }  // extern "C"
+
+// ============================================== learned start (library form)
+// The network's forward pass and the learned-start solve in C++, so a C
+// caller needs no Python: RL `pre` iterations, the U-Net's prediction, RL
+// resumed from it.  The domain transforms around the network are fused into
+// its first and last kernels: the input layer reads log(x/m + 0.01) on the
+// fly, and the head writes the advanced estimate m ((x/m + 0.01) e^r - 0.01),
+// clamped at 0, instead of r (m = mean(x), an FP64 device reduction).  No
+// host round trip and no other kernel sits between the RL iterate and the
+// resumed RL.
+namespace clarity {
+namespace nn {
+
+constexpr float kDomainEps = 0.01f;
+
+// The network's layers in the order of the FP32 parameter vector: for each,
+// weights [co][27][c1 + c2] then bias [co]; then the head (16 weights, 1 bias).
+// Index: 0 l0a (1 -> 16, SIMT), 1 l0b, 2 l1a, 3 l1b, 4 l2a, 5 l2b, 6 l3a,
+// 7 l3b, 8 l2c (skip 64 + up 128), 9 l2d, 10 l1c (32 + 64), 11 l1d,
+// 12 l0c (16 + 32), 13 l0d.
+struct NetLayer {
+  int c1, c2, co;
+};
+constexpr NetLayer kNet[14] = {{1, 0, 16},    {16, 0, 16},  {16, 0, 32},  {32, 0, 32},
+                               {32, 0, 64},   {64, 0, 64},  {64, 0, 128}, {128, 0, 128},
+                               {64, 128, 64}, {64, 0, 64},  {32, 64, 32}, {32, 0, 32},
+                               {16, 32, 16},  {16, 0, 16}};
+
+inline long long layer_weights(int l) {
+  return (long long)kNet[l].co * 27 * (kNet[l].c1 + kNet[l].c2);
+}
+// Offset of layer l's weights in the parameter vector (its bias follows).
+inline long long layer_offset(int l) {
+  long long o = 0;
+  for (int i = 0; i < l; ++i) o += layer_weights(i) + kNet[i].co;
+  return o;
+}
+
+// FP64 partial sums of x, then m = max(sum / V, 1e-20) as float.
+__global__ void k_nn_sum(const float* __restrict__ x, long long V, double* __restrict__ partial) {
+  double acc = 0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x)
+    acc += (double)x[v];
+  block_sum_store(acc, partial);
+}
+__global__ void k_nn_mean(const double* partial, int np, long long V, float* mean) {
+  const double t = block_total(partial, np);
+  if (threadIdx.x == 0) mean[0] = fmaxf((float)(t / (double)V), 1e-20f);
+}
+
+// Input layer on the log-domain input read on the fly: in(v) = log(x/m +
+// 0.01) inside the volume, 0 outside (zero padding of the transformed
+// input, as the separate transform + k_conv_in computes it).
+__global__ void k_conv_in_log(const float* __restrict__ x, int D, int H, int W,
+                              const float* __restrict__ w, const float* __restrict__ b,
+                              const float* __restrict__ mean, bf16* __restrict__ y) {
+  __shared__ float ws[16 * 27 + 16];
+  for (int i = threadIdx.x; i < 16 * 27; i += blockDim.x) ws[i] = w[i];
+  for (int i = threadIdx.x; i < 16; i += blockDim.x) ws[16 * 27 + i] = b[i];
+  __syncthreads();
+  const float m = *mean;
+  const long long V = (long long)D * H * W;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int xx = (int)(v % W);
+    const long long zy = v / W;
+    const int yy = (int)(zy % H), zz = (int)(zy / H);
+    float in[27];
+    for (int t = 0; t < 27; ++t) {
+      int dz, dy, dx;
+      tap_offset(t, &dz, &dy, &dx);
+      const int z2 = zz + dz, y2 = yy + dy, x2 = xx + dx;
+      in[t] = (z2 < 0 || y2 < 0 || x2 < 0 || z2 >= D || y2 >= H || x2 >= W)
+                  ? 0.f
+                  : logf(x[((long long)z2 * H + y2) * W + x2] / m + kDomainEps);
+    }
+    for (int co = 0; co < 16; co += 2) {
+      float r0 = ws[16 * 27 + co], r1 = ws[16 * 27 + co + 1];
+      for (int t = 0; t < 27; ++t) {
+        r0 += ws[co * 27 + t] * in[t];
+        r1 += ws[(co + 1) * 27 + t] * in[t];
+      }
+      *reinterpret_cast<__nv_bfloat162*>(y + v * 16 + co) =
+          __floats2bfloat162_rn(fmaxf(r0, 0.f), fmaxf(r1, 0.f));
+    }
+  }
+}
+
+// Head with the prediction: r = b + sum_c w[c] y[v][c];
+// out[v] = max(0, m ((x[v]/m + 0.01) e^r - 0.01)).
+__global__ void k_head_predict(const bf16* __restrict__ y, long long V, const float* __restrict__ w,
+                               const float* __restrict__ b, const float* __restrict__ x,
+                               const float* __restrict__ mean, float* __restrict__ out) {
+  const float m = *mean;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V;
+       v += (long long)gridDim.x * blockDim.x) {
+    float r = b[0];
+    for (int c = 0; c < 16; ++c) r += w[c] * __bfloat162float(y[v * 16 + c]);
+    const float p = m * ((x[v] / m + kDomainEps) * expf(r) - kDomainEps);
+    out[v] = fmaxf(p, 0.f);
+  }
+}
+
+constexpr int kMeanBlocks = 592;
+
+inline size_t round_up(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace nn
+
+long long nn_param_count() {
+  return nn::layer_offset(14) + 16 + 1;
+}
+
+#ifndef CL_CHECK
+#define CL_CHECK(call)                                         \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return status_from_cuda(e_, #call); \
+  } while (0)
+#endif
+#ifndef CL_TRY
+#define CL_TRY(expr)         \
+  do {                       \
+    Status s_ = (expr);      \
+    if (!s_.ok()) return s_; \
+  } while (0)
+#endif
+
+#define NN_TRY(expr)                                                   \
+  do {                                                                 \
+    const ClarityResult_t r_ = (expr);                                 \
+    if (r_ != CLARITY_SUCCESS) {                                       \
+      Status s_;                                                       \
+      s_.code = r_;                                                    \
+      s_.msg = std::string("network: ") + #expr;                       \
+      return s_;                                                       \
+    }                                                                  \
+  } while (0)
+
+Status nn_predict(Context& ctx, const float* params, const float* x, int D, int H, int W,
+                  float* out) {
+  using namespace nn;
+  if (D % 8 || H % 8 || W % 8) {
+    Status s;
+    s.code = CLARITY_INVALID_ARGUMENT;
+    s.msg = "learned start: volume dimensions must be multiples of 8 (three poolings)";
+    return s;
+  }
+  const long long V = (long long)D * H * W;
+  // scratch: partials | mean | BF16 weights of layers 1..13 | activations
+  size_t off = 0;
+  const size_t o_part = off;
+  off = round_up(off + sizeof(double) * kMeanBlocks);
+  const size_t o_mean = off;
+  off = round_up(off + sizeof(float));
+  size_t o_w[14] = {};
+  for (int l = 1; l < 14; ++l) {
+    o_w[l] = off;
+    off = round_up(off + sizeof(bf16) * (size_t)layer_weights(l));
+  }
+  // activations per level: three buffers at full resolution (16 ch), three
+  // at 1/2 (32 ch), three at 1/4 (64 ch), two at 1/8 (128 ch)
+  const long long lv[4] = {V * 16, V / 8 * 32, V / 64 * 64, V / 512 * 128};
+  const int nbuf[4] = {3, 3, 3, 2};
+  size_t o_a[4][3] = {};
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < nbuf[k]; ++j) {
+      o_a[k][j] = off;
+      off = round_up(off + sizeof(bf16) * (size_t)lv[k]);
+    }
+  void* base = nullptr;
+  CL_TRY(ctx.aux_scratch(off, &base));
+  char* sc = static_cast<char*>(base);
+  double* part = reinterpret_cast<double*>(sc + o_part);
+  float* mean = reinterpret_cast<float*>(sc + o_mean);
+  bf16* wf[14] = {};
+  for (int l = 1; l < 14; ++l) wf[l] = reinterpret_cast<bf16*>(sc + o_w[l]);
+  auto act = [&](int k, int j) { return reinterpret_cast<bf16*>(sc + o_a[k][j]); };
+  cudaStream_t st = ctx.exec_stream();
+  void* sv = static_cast<void*>(st);
+  // BF16 forward weights from the FP32 parameters
+  for (int l = 1; l < 14; ++l)
+    NN_TRY(clarityx_nn_pack_weights(params + layer_offset(l), kNet[l].co,
+                                    kNet[l].c1 + kNet[l].c2, wf[l], nullptr, sv));
+  // m = mean(x)
+  note_launch_begin(KK_OTHER, st);
+  CLARITY_LAUNCH(k_nn_sum, kMeanBlocks, 256, 0, st)(x, V, part);
+  CLARITY_LAUNCH(k_nn_mean, 1, 256, 0, st)(part, kMeanBlocks, V, mean);
+  CLARITY_LAUNCH(k_conv_in_log, grid_for(V), 256, 0, st)(x, D, H, W, params + layer_offset(0),
+                                                         params + layer_offset(0) +
+                                                             layer_weights(0),
+                                                         mean, act(0, 0));
+  note_launch_end(KK_OTHER, st);
+  CL_CHECK(cudaGetLastError());
+  auto conv = [&](int l, const bf16* x1, const bf16* x2, int d, int h, int w, bf16* y) {
+    return clarityx_nn_conv3(x1, kNet[l].c1, x2, kNet[l].c2, d, h, w, wf[l],
+                             params + layer_offset(l) + layer_weights(l), kNet[l].co, 1,
+                             nullptr, y, sv);
+  };
+  auto pool = [&](const bf16* a, int c, int d, int h, int w, bf16* y) {
+    return clarityx_nn_pool2(a, c, d, h, w, y, sv);
+  };
+  const int d0 = D, h0 = H, w0 = W, d1 = D / 2, h1 = H / 2, w1 = W / 2, d2 = D / 4, h2 = H / 4,
+            w2 = W / 4, d3 = D / 8, h3 = H / 8, w3 = W / 8;
+  // encoder: a0 -> s0 (kept) -> p0 -> a1 -> s1 (kept) -> p1 -> a2 -> s2 (kept) -> p2
+  NN_TRY(conv(1, act(0, 0), nullptr, d0, h0, w0, act(0, 1)));   // s0
+  NN_TRY(pool(act(0, 1), 16, d0, h0, w0, act(1, 0)));            // p0
+  NN_TRY(conv(2, act(1, 0), nullptr, d1, h1, w1, act(1, 2)));   // a1
+  NN_TRY(conv(3, act(1, 2), nullptr, d1, h1, w1, act(1, 1)));   // s1
+  NN_TRY(pool(act(1, 1), 32, d1, h1, w1, act(2, 0)));            // p1
+  NN_TRY(conv(4, act(2, 0), nullptr, d2, h2, w2, act(2, 2)));   // a2
+  NN_TRY(conv(5, act(2, 2), nullptr, d2, h2, w2, act(2, 1)));   // s2
+  NN_TRY(pool(act(2, 1), 64, d2, h2, w2, act(3, 0)));            // p2
+  NN_TRY(conv(6, act(3, 0), nullptr, d3, h3, w3, act(3, 1)));   // a3
+  NN_TRY(conv(7, act(3, 1), nullptr, d3, h3, w3, act(3, 0)));   // b3
+  // decoder: skip + nearest-upsampled coarse tensor, read inside the loader
+  NN_TRY(conv(8, act(2, 1), act(3, 0), d2, h2, w2, act(2, 0)));  // c2
+  NN_TRY(conv(9, act(2, 0), nullptr, d2, h2, w2, act(2, 2)));    // d2
+  NN_TRY(conv(10, act(1, 1), act(2, 2), d1, h1, w1, act(1, 0))); // c1
+  NN_TRY(conv(11, act(1, 0), nullptr, d1, h1, w1, act(1, 2)));   // d1
+  NN_TRY(conv(12, act(0, 1), act(1, 2), d0, h0, w0, act(0, 0))); // c0
+  NN_TRY(conv(13, act(0, 0), nullptr, d0, h0, w0, act(0, 2)));   // d0
+  const float* head = params + layer_offset(14);
+  note_launch_begin(KK_OTHER, st);
+  CLARITY_LAUNCH(k_head_predict, grid_for(V), 256, 0, st)(act(0, 2), V, head, head + 16, x, mean,
+                                                          out);
+  note_launch_end(KK_OTHER, st);
+  CL_CHECK(cudaGetLastError());
+  return Status::Ok();
+}
+
+Status run_ml_learned(Context& ctx, const float* img, Dims id, const float* ker, Dims kd,
+                      const float* params, int pre, float* out, int post, double* idiv) {
+  if (id.x % 8 || id.y % 8 || id.z % 8) {
+    Status s;
+    s.code = CLARITY_INVALID_ARGUMENT;
+    s.msg = "learned start: image dimensions must be multiples of 8 (three poolings)";
+    return s;
+  }
+  if (pre < 0 || post < 0) {
+    Status s;
+    s.code = CLARITY_INVALID_ARGUMENT;
+    s.msg = "learned start: pre and post must be >= 0";
+    return s;
+  }
+  // the early iterate and the prediction live in the workspace's spare
+  // volumes (accelerated-RL buffers, allocated on first use)
+  const PlanEntry* pe;
+  CL_TRY(ctx.plan(Dims{id.x + kd.x, id.y + kd.y, id.z + kd.z}, &pe));
+  Workspace* ws;
+  CL_TRY(ctx.workspace(*pe, id, kd, &ws));
+  const long long n = id.n();
+  if (ws->xbuf_cap < n) {
+    for (float*& b : ws->xbuf) {
+      cudaFree(b);
+      b = nullptr;
+    }
+    ws->xbuf_cap = 0;
+    for (float*& b : ws->xbuf) CL_CHECK(dev_alloc((void**)&b, sizeof(float) * (size_t)n));
+    ws->xbuf_cap = n;
+  }
+  float* early = ws->xbuf[0];
+  float* start = ws->xbuf[1];
+  CL_TRY(run_rl_ex(ctx, img, id, ker, kd, nullptr, early, pre, nullptr));
+  CL_TRY(nn_predict(ctx, params, early, id.z, id.y, id.x, start));
+  return run_rl_ex(ctx, img, id, ker, kd, start, out, post, idiv);
+}
+
+}  // namespace clarity

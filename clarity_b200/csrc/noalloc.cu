@@ -2,10 +2,11 @@
 // memory at all (clarityx_convolve_noalloc, include/clarity_ext.h).
 //
 // Why it exists: some callers must not allocate device memory once they are
-// running -- code that records its work into a CUDA graph or runs under a
-// memory pool it manages itself, real-time loops whose memory use must be
-// fixed up front, and plugins hosted inside another process's CUDA context
-// that forbids cudaMalloc.  The regular entry points allocate their spectra
+// running -- code that runs under a memory pool it manages itself (a
+// cudaMalloc behind the pool's back breaks its accounting), real-time loops
+// whose memory use must be fixed up front (an allocation can stall or fail
+// mid-run), and plugins hosted inside another process's CUDA context that
+// forbids cudaMalloc.  The regular entry points allocate their spectra
 // and plan tables on first use; this one keeps every scratch buffer (OTF,
 // work spectrum, twiddle and digit-reversal tables) in one file-scope
 // __device__ array of kScratchBytes.  Every GPU that loads the library holds
@@ -26,8 +27,11 @@
 namespace clarity {
 namespace {
 
-// 32 MiB: the OTF and the work spectrum of a padded work box of up to
-// 128 x 128 x 128 voxels, plus the plan tables.
+// 32 MiB: the plan tables, the OTF and the work spectrum.  The limit is in
+// bytes, not in a box shape: a work box fits when its two spectra
+// (2 x spec_elems x 8 bytes, spec_elems from clarityx_plan_info) and tables
+// do -- 128 x 128 x 128 (16.5 MiB) and 128 x 128 x 192 (24.4 MiB) fit,
+// 256 x 256 x 256 does not.
 constexpr size_t kScratchBytes = size_t(32) << 20;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -36,16 +40,17 @@ std::mutex g_addr_mu;
 void* g_addr[kMaxDevices] = {};
 
 struct Tables {
-  TwTable t[5];
-  int ntab;
+  TwTable t[kPlanTwTables];
 };
 
-// Twiddles in FP64 (sincospi), rounded; the digit-reversed x slot table.
+// Twiddles in FP64 (sincospi), rounded; the digit-reversed x slot table.  The
+// tables are the planner's own (plan_twiddle_tables, xrev_slot), as the
+// cached plans of the other entry points build them.
 __global__ void k_noalloc_tables(float2* tw, Tables tabs, int* xrev, AxisPlan ax,
                                  int M) {
   const int stride = gridDim.x * blockDim.x;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int k = 0; k < tabs.ntab; ++k) {
+  for (int k = 0; k < kPlanTwTables; ++k) {
     const TwTable T = tabs.t[k];
     for (int t = t0; t < T.count; t += stride) {
       double s, c;
@@ -53,15 +58,7 @@ __global__ void k_noalloc_tables(float2* tw, Tables tabs, int* xrev, AxisPlan ax
       tw[T.off + t] = make_float2((float)c, (float)(-s));
     }
   }
-  for (int k = t0; k < M; k += stride) {
-    int rem = k, pos = 0;
-    for (int s = 0; s < ax.npass; ++s) {
-      const int d = rem % ax.radix[s];
-      rem /= ax.radix[s];
-      pos += d * ax.span[s];
-    }
-    xrev[k] = pos;
-  }
+  for (int k = t0; k < M; k += stride) xrev[k] = xrev_slot(ax, k);
 }
 
 size_t round256(size_t v) { return (v + 255) & ~size_t(255); }
@@ -71,9 +68,13 @@ ClarityResult_t fail(ClarityResult_t code, const char* msg) {
   return code;
 }
 
-// Device address of the scratch array on the current device.  Looked up
-// once per device with that device current (in host code the array's name
-// is only a host-side stand-in, not a device address).
+// Device address of the scratch array on the current device.  In host code
+// the array's name is only a host-side stand-in, not a device address, so
+// the first call on each device looks the address up (cudaGetSymbolAddress)
+// with that device current and keeps it for the life of the process.  That
+// first call should therefore come before any stream capture, and the entry
+// point must not be used after cudaDeviceReset (which would invalidate the
+// kept address).
 cudaError_t scratch_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -130,6 +131,7 @@ extern "C" CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
                   nx, ny, nz, need, kScratchBytes);
     return fail(CLARITY_INVALID_ARGUMENT, msg);
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   void* base = nullptr;
   cudaError_t e = scratch_address(&base);
   if (e != cudaSuccess) return fail(CLARITY_INVALID_OPERATION, cudaGetErrorString(e));
@@ -138,15 +140,9 @@ extern "C" CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
   int* xrev = reinterpret_cast<int*>(sc + off_rev);
   float2* H = reinterpret_cast<float2*>(sc + off_h);
   float2* S = reinterpret_cast<float2*>(sc + off_s);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
 
   Tables tabs;
-  tabs.ntab = 5;
-  tabs.t[0] = {P.ax.tw_off, P.M > 1 ? P.M : 1, P.M > 1 ? P.M : 1};
-  tabs.t[1] = {P.ayB.tw_off, P.By > 1 ? P.By : 1, P.By > 1 ? P.By : 1};
-  tabs.t[2] = {P.az.tw_off, P.nz > 1 ? P.nz : 1, P.nz > 1 ? P.nz : 1};
-  tabs.t[3] = {P.tw_r2c_off, P.nx, P.M / 2 + 1};
-  tabs.t[4] = {P.tw_ny_off, P.ny, P.ny};
+  plan_twiddle_tables(P, tabs.t);
   CLARITY_LAUNCH(k_noalloc_tables, 64, 256, 0, st)(tw, tabs, xrev, P.ax, P.M);
 
   const Dims wd{nx, ny, nz};

@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(256, 2)
     static_assert((BW * 8) % 16 == 0 && (ZS * 8) % 16 == 0 && (SH::TILE * 8) % 16 == 0,
                   "bulk copies need 16-byte sizes and offsets");
     if (!smem_aligned16(sm)) {  // never expected: refuse rather than fault
-      if (threadIdx.x == 0) atomicExch(T.err, kErrMisaligned);
+      if (threadIdx.x == 0) raise_error(T.err, kErrMisaligned);
       return;
     }
     if (threadIdx.x == 0) mbar_init(&bar, 1);

@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(256, 3)
     return;
   }
   if (!smem_aligned128(buf)) {    // never expected: refuse rather than fault
-    if (threadIdx.x == 0) atomicExch(T.err, kErrMisaligned);
+    if (threadIdx.x == 0) raise_error(T.err, kErrMisaligned);
     return;
   }
   if (threadIdx.x == 0) {

@@ -69,12 +69,43 @@ struct VolPlan {
   long long n_real() const { return (long long)nx * ny * nz; }
 };
 
+#if defined(__CUDACC__) && !defined(CLARITY_HOST_EMULATION)
+#define CLARITY_HD __host__ __device__
+#else
+#define CLARITY_HD
+#endif
+
 // Twiddle table w_n^t = exp(-2 pi i t / n), t < count, at float2 offset off.
 struct TwTable {
   int off, n, count;
 };
-// The digit-reversed slot of each natural x frequency after the x DIF
-// passes, and the twiddle tables a plan needs.
+constexpr int kPlanTwTables = 5;
+
+// The smem slot of natural x frequency k after the x DIF passes (digits of
+// k in the passes' radices, each times its pass's span).
+CLARITY_HD inline int xrev_slot(const AxisPlan& ax, int k) {
+  int rem = k, pos = 0;
+  for (int s = 0; s < ax.npass; ++s) {
+    const int d = rem % ax.radix[s];
+    rem /= ax.radix[s];
+    pos += d * ax.span[s];
+  }
+  return pos;
+}
+
+// The twiddle tables a plan needs (x, y0 and z passes, the r2c split, the y
+// split), kPlanTwTables of them; fills `out` without allocating.
+inline void plan_twiddle_tables(const VolPlan& P, TwTable out[kPlanTwTables]) {
+  const int m = P.M > 1 ? P.M : 1, by = P.By > 1 ? P.By : 1, nz = P.nz > 1 ? P.nz : 1;
+  out[0] = TwTable{P.ax.tw_off, m, m};
+  out[1] = TwTable{P.ayB.tw_off, by, by};
+  out[2] = TwTable{P.az.tw_off, nz, nz};
+  out[3] = TwTable{P.tw_r2c_off, P.nx, P.M / 2 + 1};
+  out[4] = TwTable{P.tw_ny_off, P.ny, P.ny};
+}
+
+// The digit-reversed slot of each natural x frequency (xrev_slot), and the
+// twiddle tables (plan_twiddle_tables), as vectors.
 void plan_tables(const VolPlan& P, std::vector<int>* xrev, std::vector<TwTable>* tabs);
 
 // Planner (host only).  Returns false for shapes it cannot decompose.

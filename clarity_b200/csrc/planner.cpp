@@ -193,22 +193,10 @@ int make_plan_candidates(int nx, int ny, int nz, VolPlan* out, int max_out, std:
 
 void plan_tables(const VolPlan& P, std::vector<int>* xrev, std::vector<TwTable>* tabs) {
   xrev->assign(std::max(P.M, 1), 0);
-  for (int k = 0; k < P.M; ++k) {
-    int rem = k, pos = 0;
-    for (int s = 0; s < P.ax.npass; ++s) {
-      const int d = rem % P.ax.radix[s];
-      rem /= P.ax.radix[s];
-      pos += d * P.ax.span[s];
-    }
-    (*xrev)[k] = pos;
-  }
-  *tabs = {
-      {P.ax.tw_off, std::max(P.M, 1), std::max(P.M, 1)},
-      {P.ayB.tw_off, std::max(P.By, 1), std::max(P.By, 1)},
-      {P.az.tw_off, std::max(P.nz, 1), std::max(P.nz, 1)},
-      {P.tw_r2c_off, P.nx, P.M / 2 + 1},
-      {P.tw_ny_off, P.ny, P.ny},
-  };
+  for (int k = 0; k < P.M; ++k) (*xrev)[k] = xrev_slot(P.ax, k);
+  TwTable t[kPlanTwTables];
+  plan_twiddle_tables(P, t);
+  tabs->assign(t, t + kPlanTwTables);
 }
 
 }  // namespace clarity

@@ -193,13 +193,31 @@ __device__ __forceinline__ void prefetch_l2_range(const void* begin, size_t byte
 bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
                           const unsigned long long stride_bytes[3], const unsigned box[4]);
 
-// Bounded wait for phase `parity` of the barrier; false (and *err set) on
-// timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  for (long long it = 0; it < kWaitLimit; ++it)
+// Records `code` in the context's error word.  The word lives in mapped
+// pinned host memory (the host reads it without synchronising the device),
+// so it is written with a plain volatile store and a system-scope fence, not
+// an atomic: any nonzero code means "this call's result is not valid".
+__device__ __forceinline__ void raise_error(int* err, int code) {
+  if (!err) return;
+  *reinterpret_cast<volatile int*>(err) = code;
+#ifndef CLARITY_HOST_EMULATION
+  __threadfence_system();
+#endif
+}
+
+// Bounded wait for phase `parity` of the barrier: at most `limit` polls of
+// mbarrier.try_wait; false (and `code` kErrWaitTimeout in *err) when it gives up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err,
+                                                  long long limit) {
+  for (long long it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
-  if (err) atomicExch(err, kErrWaitTimeout);
+  raise_error(err, kErrWaitTimeout);
   return false;
+}
+
+// Bounded wait with the library's limit (kWaitLimit polls).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  return mbar_wait_bounded(bar, parity, err, kWaitLimit);
 }
 
 }  // namespace clarity

@@ -116,10 +116,14 @@ def learned_solve(net: unet.UNet3D, img_d, psf_d, out, post: int, pre: int | Non
     """RL `pre` iterations (default: the iterate the network was trained on),
     the network's prediction, RL resumed for `post` iterations from it --
     plain, or accelerated (Biggs-Andrews) with accel (idiv: trace of the
-    resumed part, post + 1 entries)."""
+    resumed part, post + 1 entries).  The plain form is one library call
+    (clarityx_ml_learned_device)."""
     import torch
     if pre is None:
         pre = getattr(net, "pre", PRE)
+    if not accel:
+        return api.ml_learned_device(img_d, psf_d, net.p, out, pre, post, idiv=idiv,
+                                     stream=stream)
     early = torch.empty_like(img_d)
     api.ml_device(img_d, psf_d, early, pre, stream)
     start = unet.predict(net, early, stream=stream).contiguous()

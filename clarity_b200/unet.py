@@ -300,7 +300,18 @@ def apply_prediction(x_early, r):
 
 
 def predict(net: UNet3D, x_early, stream=None):
-    """The network's advanced estimate from an early iterate."""
+    """The network's advanced estimate from an early iterate, by the
+    library's fused forward (clarityx_nn_predict: the domain transforms run
+    inside the network's first and last kernels)."""
+    import torch
+    out = torch.empty_like(x_early)
+    return api.nn_predict(net.p, x_early.contiguous(), out, stream=stream)
+
+
+def predict_unfused(net: UNet3D, x_early, stream=None):
+    """The same prediction through the training path's separate domain
+    transforms (to_input, forward, apply_prediction): the check for the
+    fused form."""
     inp, _ = to_input(x_early)
     r = net.forward(inp, stream=stream)
     return apply_prediction(x_early, r)

@@ -6,8 +6,18 @@
  * and host-side fault injection for tests.
  *
  * Device-pointer functions: every pointer is a CUDA device pointer on the
- * library's device; `stream` is a cudaStream_t (NULL = the library's own
- * stream).  They are asynchronous with respect to the host unless stated.
+ * library's device; `stream` is a cudaStream_t and work is enqueued on it
+ * (NULL is the legacy default stream, so the work is ordered with the
+ * caller's other default-stream work).  They are asynchronous with respect to
+ * the host unless stated.
+ *
+ * Failure detection: the fused passes wait for their tile copies with
+ * bounded waits.  A wait that gives up records the failure in the library's
+ * error word (mapped host memory, readable without synchronising) and the
+ * kernel returns.  clarityx_synchronize reports it; so does the next call
+ * into the library, which then returns CLARITY_INVALID_OPERATION without
+ * enqueuing anything (the failed call's result is not valid).  The word is
+ * cleared once reported.
  */
 #ifndef CLARITY_B200_CLARITY_EXT_H_
 #define CLARITY_B200_CLARITY_EXT_H_
@@ -30,9 +40,19 @@ CLARITY_API void clarityx_inject_device_alloc_failure(int countdown);
 /* Releases cached work buffers (plans stay cached). */
 CLARITY_API ClarityResult_t clarityx_trim(void);
 
-/* Blocks until all work the library enqueued has finished; returns the
- * first asynchronous error as a result code. */
+/* Blocks until `stream` has finished (NULL: every stream of the library's
+ * device, the library's own included), then returns the first asynchronous
+ * error as a result code: a CUDA error, or CLARITY_INVALID_OPERATION when a
+ * device-side bounded wait gave up (see above). */
 CLARITY_API ClarityResult_t clarityx_synchronize(void *stream);
+
+/* Failure-detection self test: enqueues on `stream` a one-thread kernel that
+ * arms an mbarrier for bytes no copy will deliver and waits on it with a
+ * short bound (about a millisecond).  The wait gives up and records a
+ * timeout exactly as a fused pass's would, so the next clarityx_synchronize
+ * or library call reports CLARITY_INVALID_OPERATION.  No copy is issued and
+ * the GPU stays usable.  For tests of callers' error handling. */
+CLARITY_API ClarityResult_t clarityx_inject_wait_timeout(void *stream);
 
 /* Device-resident versions of the public algorithms.  image/kernel/out are
  * unpadded device volumes of imageDim / kernelDim / imageDim voxels. */
@@ -45,6 +65,24 @@ CLARITY_API ClarityResult_t clarityx_wiener_device(
 CLARITY_API ClarityResult_t clarityx_ml_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+/* Conjugate-for-correlation opt-ins (no reference counterpart; the
+ * reference never conjugates the OTF, src/MaximumLikelihoodDeconvolve.cxx
+ * :57,65 and src/ModulateGPU.cu:63-72).  clarityx_correlate_device is
+ * clarityx_convolve_device with the kernel's spectrum conjugated in the z
+ * pass: the circular correlation with the kernel.
+ * clarityx_ml_correlate_device is clarityx_ml_device whose second
+ * convolution per iteration (the reference's h * (g / (h * u))) is that
+ * correlation -- the h^T of the textbook Richardson-Lucy update.  The two
+ * forms agree for a kernel symmetric about its centre; for the 256x256x64
+ * halo PSF (|Im H| / |H| ~ 1e-4) they differ by more than the reference
+ * parity tolerance, so the reference form stays the default. */
+CLARITY_API ClarityResult_t clarityx_correlate_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, void *stream);
+CLARITY_API ClarityResult_t clarityx_ml_correlate_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);
+
 /* Blind ML with the PSF update that Clarity_BlindMaximumLikelihoodDeconvolve
  * leaves disabled (src/BlindMaximumLikelihoodDeconvolve.cxx:96): per outer
  * iteration one object step o <- o (h * (g / (h * o))), then
@@ -146,21 +184,30 @@ CLARITY_API ClarityResult_t clarityx_plan_info(Clarity_Dim3 workDim,
 /* Circular convolution of device buffers that allocates nothing (no
  * cudaMalloc, cudaFree or allocating library call; no Clarity_Register
  * needed).  It has no counterpart in the reference.  It is for callers that
- * cannot allocate device memory once running: work recorded into CUDA graphs
- * or run under the caller's own memory pool, fixed-footprint real-time
- * loops, and plugins hosted in a context that forbids cudaMalloc.
+ * cannot allocate device memory once running: code that runs under a memory
+ * pool it manages itself (an allocation behind the pool's back breaks its
+ * accounting), real-time loops whose footprint must be fixed up front (an
+ * allocation can stall or fail mid-run), and plugins hosted in a context
+ * that forbids cudaMalloc.
  * image/kernel/out are device buffers on the current device, as in
- * clarityx_convolve_device, and the result is the same.
+ * clarityx_convolve_device, and the result is the same.  Work is enqueued
+ * on `stream` (NULL: the legacy default stream, as for every _device call);
+ * no library stream or registration is involved.
  * Scratch: one 32 MiB array in the library's device memory (held by every
- * GPU that loads the library until exit), enough for a padded work box of
- * 128 x 128 x 128 voxels; larger boxes return CLARITY_INVALID_ARGUMENT
- * with the size needed in clarityx_last_error().  The first call on each
- * device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.
- * Every call shares the one array: calls that overlap on the GPU (two
- * streams, two host threads) race and corrupt each other's results, so
- * serialise them.  Nothing in the array needs to start at zero; each call
- * rewrites what it reads. */
+ * GPU that loads the library until exit).  The limit is in bytes: the work
+ * box (image + kernel per axis) fits when its OTF and work spectrum
+ * (2 x spec_elems x 8 bytes; spec_elems is field 15 of clarityx_plan_info,
+ * in units of 1024) plus the plan tables fit in 32 MiB -- a 64^3 image with a
+ * 64^3 kernel (work box 128^3, 16.5 MiB) fits, 128 x 128 x 192 (24.4 MiB)
+ * fits, 256 x 256 x 256 does not.  A box that does not fit returns
+ * CLARITY_INVALID_ARGUMENT with the size needed in clarityx_last_error().
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current) and keeps it for the
+ * life of the process: make that first call before any stream capture, and
+ * do not use this entry point after cudaDeviceReset.  Every call shares the
+ * one array: calls that overlap on the GPU (two streams, two host threads)
+ * race and corrupt each other's results, so serialise them.  Nothing in the
+ * array needs to start at zero; each call rewrites what it reads. */
 CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, void *stream);
@@ -220,6 +267,33 @@ CLARITY_API ClarityResult_t clarityx_nn_adam(float *p, const float *g, float *m,
                                              float eps, int step, void *stream);
 CLARITY_API ClarityResult_t clarityx_nn_pack_weights(const float *w, int cout, int cin,
                                                      void *wf, void *wb, void *stream);
+
+/* Learned start as one call (no reference counterpart): RL `pre` iterations
+ * (clarityx_ml_device), the learned-start network's prediction of an advanced
+ * estimate from that iterate, then RL resumed from the prediction for `post`
+ * iterations (clarityx_ml_ex_device with a start; idiv as there, post + 1
+ * entries).  The network is the 3-D U-Net the kernels below implement (4
+ * levels, widths 16-32-64-128, BF16 tensor-core convolutions, FP32
+ * accumulation); `params` is its FP32 parameter vector on the device,
+ * nparams = clarityx_nn_param_count() floats in the order of
+ * clarity_b200/unet.py (clarity_b200/learned_start_weights.npy holds trained
+ * ones).  Around the network the estimate is taken to the log domain and
+ * back inside its first and last kernels: input log(x/m + 0.01), prediction
+ * max(0, m ((x/m + 0.01) e^r - 0.01)) with m = mean(x).  Image dimensions
+ * must be multiples of 8.  Device pointers, asynchronous on `stream`. */
+CLARITY_API ClarityResult_t clarityx_ml_learned_device(
+    const float *image, Clarity_Dim3 imageDim, const float *kernel,
+    Clarity_Dim3 kernelDim, const float *params, long long nparams, int pre,
+    float *out, int post, double *idiv, void *stream);
+/* The network's prediction alone: out = max(0, m ((x/m + 0.01) e^r - 0.01)),
+ * r = U-Net(log(x/m + 0.01)), for a volume x of `dim` voxels (multiples of
+ * 8).  Needs Clarity_Register (its activations live in the library's
+ * cached scratch). */
+CLARITY_API ClarityResult_t clarityx_nn_predict(const float *params, long long nparams,
+                                                const float *x, Clarity_Dim3 dim, float *out,
+                                                void *stream);
+/* Length of the network's FP32 parameter vector. */
+CLARITY_API long long clarityx_nn_param_count(void);
 
 /* Benchmark probes.  clarityx_launch_count: kernels the library has
  * launched so far.  clarityx_timing_enable(1) makes every fused-pass launch

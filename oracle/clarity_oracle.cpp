@@ -136,15 +136,26 @@ T reduce_sum(const T* a, long n, int mode) {
   return (T)s;
 }
 
-// Clarity_Convolve: src/Convolve.cxx:41-115,146-184.
+// conj(v) in place: the spectrum of the reflected kernel, h(-x), so that a
+// product with it is a correlation with h (no reference counterpart: the
+// reference never conjugates, src/MaximumLikelihoodDeconvolve.cxx:57,65).
+template <class T>
+void conjugate(std::vector<oracle::cx<T>>& v) {
+  for (auto& c : v) c = oracle::cx<T>(c.real(), -c.imag());
+}
+
+// Clarity_Convolve: src/Convolve.cxx:41-115,146-184.  correlate: the
+// kernel's spectrum is conjugated first (circular correlation; an opt-in of
+// this library with no reference counterpart).
 template <class T, class S>
 void convolve(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out,
-              T* out_work) {
+              T* out_work, bool correlate = false) {
   Work<T> w(in, id, kernel, kd);
   std::vector<oracle::cx<T>> a(w.nc), b(w.nc);
   std::vector<T> o(w.n);
   w.r2c(w.g.data(), a.data());
   w.r2c(w.h.data(), b.data());
+  if (correlate) conjugate<T>(b);
   modulate<T>(w.nc, a.data(), b.data(), inv_n<T>(w.wd), a.data());
   w.c2r(a.data(), o.data());
   clip<T, S>(out, id, o.data(), w.wd);
@@ -180,13 +191,23 @@ double idiv_image(const Work<T>& w, Dim3 id, const T* b) {
 // first estimate (an image-sized volume, zero-padded like the image); `idiv`
 // receives, per iteration, the I-divergence of the image against s1 = h * u
 // over the image region (the definition of oracle_idivergence, in double).
+//
+// correlate (no reference counterpart): the second convolution of every
+// iteration (:65) uses the conjugated OTF -- a correlation with h, the
+// textbook h^T of Richardson-Lucy -- instead of the reference's h.
 template <class T, class S>
 void rl(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
-        int sum_mode, T* out_work, const S* start = nullptr, double* idiv = nullptr) {
+        int sum_mode, T* out_work, const S* start = nullptr, double* idiv = nullptr,
+        bool correlate = false) {
   Work<T> w(in, id, kernel, kd);
   const long n = w.n;
-  std::vector<oracle::cx<T>> otf(w.nc), tmp(w.nc);
+  std::vector<oracle::cx<T>> otf(w.nc), tmp(w.nc), otf2;
   w.r2c(w.h.data(), otf.data());                      // :98
+  if (correlate) {
+    otf2 = otf;
+    conjugate<T>(otf2);
+  }
+  const oracle::cx<T>* second = correlate ? otf2.data() : otf.data();
   std::vector<T> u(w.g), s1(n), s2(n);
   if (start) {
     const int zero[3] = {0, 0, 0};
@@ -202,7 +223,7 @@ void rl(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
     for (long i = 0; i < n; i++)
       s1[i] = ((double)std::fabs(s1[i]) < 1e-5) ? (T)0 : w.g[i] / s1[i];
     // :65 s2 = h * s1
-    convolve_otf<T>(w, s1.data(), otf.data(), s2.data(), tmp);
+    convolve_otf<T>(w, s1.data(), second, s2.data(), tmp);
     // :69-70 u = u * s2
     for (long i = 0; i < n; i++) u[i] = u[i] * s2[i];
     // :73-78 flux rescale over the whole padded box
@@ -571,6 +592,28 @@ void oracle_convolve_f64(const float* in, int ix, int iy, int iz,
                          double* work) {
   ORACLE_DIMS;
   convolve<double, float>(in, id, k, kd, out, work);
+}
+void oracle_correlate_f32(const float* in, int ix, int iy, int iz,
+                          const float* k, int kx, int ky, int kz, float* out) {
+  ORACLE_DIMS;
+  convolve<float, float>(in, id, k, kd, out, (float*)nullptr, true);
+}
+void oracle_correlate_f64(const float* in, int ix, int iy, int iz,
+                          const float* k, int kx, int ky, int kz, float* out) {
+  ORACLE_DIMS;
+  convolve<double, float>(in, id, k, kd, out, (double*)nullptr, true);
+}
+void oracle_rl_corr_f32(const float* in, int ix, int iy, int iz, const float* k,
+                        int kx, int ky, int kz, float* out, int iters) {
+  ORACLE_DIMS;
+  rl<float, float>(in, id, k, kd, out, iters, SUM_DOUBLE, (float*)nullptr, nullptr, nullptr,
+                   true);
+}
+void oracle_rl_corr_f64(const float* in, int ix, int iy, int iz, const float* k,
+                        int kx, int ky, int kz, float* out, int iters) {
+  ORACLE_DIMS;
+  rl<double, float>(in, id, k, kd, out, iters, SUM_DOUBLE, (double*)nullptr, nullptr, nullptr,
+                    true);
 }
 void oracle_rl_f32(const float* in, int ix, int iy, int iz, const float* k,
                    int kx, int ky, int kz, float* out, int iters,

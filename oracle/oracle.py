@@ -27,7 +27,9 @@ REF_SO = {
     "ref": os.path.join(HERE, "_ref", "liboracle_ref.so"),
     "ref_fp64sum": os.path.join(HERE, "_ref", "liboracle_ref_fp64sum.so"),
 }
-REFERENCE_DIR = os.environ.get("CLARITY_REFERENCE_DIR", "/root/reference")
+# The reference source tree the checker builds from: CLARITY_REFERENCE_DIR,
+# or the `reference_dir` argument of build().  Nothing at run time reads it.
+REFERENCE_DIR = os.environ.get("CLARITY_REFERENCE_DIR", "")
 
 SUM_SERIAL_FLOAT = 0
 SUM_DOUBLE = 1
@@ -36,13 +38,16 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
-def build(with_reference: bool | None = None) -> None:
-    """Compile the oracle (and, when the reference sources exist, _ref)."""
+def build(with_reference: bool | None = None, reference_dir: str | None = None) -> None:
+    """Compile the oracle and, when the reference sources are given and
+    present, _ref (the reference build, its test programs and app) and the
+    drop-in builds of those programs against libclarity.so (build the library
+    first)."""
+    ref = reference_dir if reference_dir is not None else REFERENCE_DIR
     if with_reference is None:
-        with_reference = os.path.isdir(os.path.join(REFERENCE_DIR, "src"))
-    targets = ["oracle"] + (["ref"] if with_reference else [])
-    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_DIR}", *targets],
-                   check=True)
+        with_reference = bool(ref) and os.path.isdir(os.path.join(ref, "src"))
+    targets = ["oracle"] + (["ref", "dropin"] if with_reference else [])
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref}", *targets], check=True)
 
 
 class _Dim3(C.Structure):
@@ -81,6 +86,10 @@ class Oracle:
                 extra64 = [i]  # no sum mode: always double
             fn64.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p] + extra64 + [C.c_void_p]
             fn64.restype = None
+        for p in ("f32", "f64"):
+            getattr(L, f"oracle_correlate_{p}").argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p]
+            getattr(L, f"oracle_rl_corr_{p}").argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p,
+                                                         i]
         L.oracle_rl_ex_f32.argtypes = [_f32p, i, i, i, _f32p, i, i, i, _f32p, i, i,
                                        C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_rl_ex_f32.restype = None
@@ -127,6 +136,24 @@ class Oracle:
 
     def convolve(self, img, psf, precision="f32", work=False):
         return self._run("convolve", img, psf, [], precision, work)
+
+    def correlate(self, img, psf, precision="f32"):
+        """Circular correlation: Clarity_Convolve with the kernel's spectrum
+        conjugated (the library's opt-in; no reference counterpart)."""
+        img, psf = _f32(img), _f32(psf)
+        out = np.empty_like(img)
+        getattr(self.lib, f"oracle_correlate_{precision}")(img, *_dims(img), psf, *_dims(psf),
+                                                           out)
+        return out
+
+    def rl_correlate(self, img, psf, iters, precision="f32"):
+        """RL whose second convolution per iteration is a correlation with
+        the kernel (conjugated OTF), double flux sums."""
+        img, psf = _f32(img), _f32(psf)
+        out = np.empty_like(img)
+        getattr(self.lib, f"oracle_rl_corr_{precision}")(img, *_dims(img), psf, *_dims(psf), out,
+                                                         int(iters))
+        return out
 
     def rl(self, img, psf, iters, precision="f32", sum_mode=SUM_DOUBLE, work=False):
         extra = [iters, sum_mode] if precision == "f32" else [iters]

@@ -105,6 +105,11 @@ int main(int argc, char** argv) {
     float* sig[3] = {&sx, &sy, &sz};
     r = Clarity_SmoothedJansenVanCittertDeconvolve(img.data(), id, psf.data(), kd, out.data(),
                                                    (unsigned)param, 2u, sig);
+  } else if (op == "correlate") {  // emulated device memory is host memory
+    r = clarityx_correlate_device(img.data(), id, psf.data(), kd, out.data(), nullptr);
+  } else if (op == "rlcorr") {
+    r = clarityx_ml_correlate_device(img.data(), id, psf.data(), kd, out.data(), (int)param,
+                                     nullptr);
   } else if (op == "accel") {  // accelerated RL, emulated device memory is host memory
     r = clarityx_ml_accel_device(img.data(), id, psf.data(), kd, nullptr, out.data(), (int)param,
                                  nullptr, nullptr);

@@ -22,6 +22,30 @@ cudaError_t cudaFree(void* p) {
   std::free(p);
   return cudaSuccess;
 }
+// mapped pinned host memory: the host pointer is the device alias
+cudaError_t cudaHostAlloc(void** p, size_t n, unsigned int) {
+  *p = std::malloc(n ? n : 16);
+  return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+cudaError_t cudaFreeHost(void* p) {
+  std::free(p);
+  return cudaSuccess;
+}
+cudaError_t cudaHostGetDevicePointer(void** d, void* h, unsigned int) {
+  *d = h;
+  return cudaSuccess;
+}
+// every host pointer is ordinary (pageable) memory in the emulation, so
+// the host API's pinned bounce path runs
+cudaError_t cudaPointerGetAttributes(cudaPointerAttributes* a, const void*) {
+  std::memset(a, 0, sizeof(*a));
+  a->type = cudaMemoryTypeUnregistered;
+  return cudaSuccess;
+}
+cudaError_t cudaStreamIsCapturing(cudaStream_t, cudaStreamCaptureStatus* s) {
+  *s = cudaStreamCaptureStatusNone;
+  return cudaSuccess;
+}
 cudaError_t cudaMemcpyAsync(void* d, const void* s, size_t n, cudaMemcpyKind, cudaStream_t) {
   std::memcpy(d, s, n);
   return cudaSuccess;

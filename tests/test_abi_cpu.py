@@ -144,3 +144,42 @@ def test_raw_image_app_usage_without_gpu():
     p = subprocess.run([app], capture_output=True, text=True)
     assert p.returncode == 1
     assert "<image filename> <x> <y> <z> <psf filename> <x> <y> <z> <output file name>" in p.stdout
+
+
+def test_network_parameter_count_matches_the_python_layout():
+    # the C forward reads the FP32 parameter vector in unet.UNet3D's order:
+    # per layer weights [co][27][c1 + c2] then bias [co], then the head
+    from clarity_b200 import learned, unet
+    specs = [("l0a", 1, 0, 16)] + unet.CONV_LAYERS
+    n = sum(co * 27 * (c1 + c2) + co for _, c1, c2, co in specs) + 16 + 1
+    assert api.nn_param_count() == n
+    assert np.load(learned.WEIGHTS).size == n
+
+
+def test_learned_start_argument_errors_without_device():
+    L = api.load()
+    d3 = api.Dim3(16, 16, 16)
+    n = api.nn_param_count()
+    rc = L.clarityx_ml_learned_device(C.c_void_p(16), d3, C.c_void_p(16), d3, None, n, 5,
+                                      C.c_void_p(16), 2, None, None)
+    assert rc == api.CLARITY_INVALID_ARGUMENT
+    rc = L.clarityx_ml_learned_device(C.c_void_p(16), d3, C.c_void_p(16), d3, C.c_void_p(16),
+                                      n - 1, 5, C.c_void_p(16), 2, None, None)
+    assert rc == api.CLARITY_INVALID_ARGUMENT
+    assert "parameters" in L.clarityx_last_error().decode()
+
+
+def test_compat_header_compiles_a_reference_style_caller(tmp_path):
+    # `#include <Clarity.h>` with include/compat on the path declares the
+    # reference's API from this library's header
+    src = tmp_path / "caller.c"
+    src.write_text('#include <Clarity.h>\n'
+                   'int main(void) { Clarity_Dim3 d = {1, 2, 3};\n'
+                   '  return Clarity_ResultString(CLARITY_SUCCESS) != 0 && d.z == 3 ? 0 : 1; }\n')
+    exe = tmp_path / "caller"
+    p = subprocess.run(["gcc", "-I", os.path.join(ROOT, "include", "compat"), str(src), "-o",
+                        str(exe), "-L", os.path.dirname(api.LIB_PATH), "-lclarity",
+                        f"-Wl,-rpath,{os.path.dirname(api.LIB_PATH)}"],
+                       capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
+    assert subprocess.run([str(exe)]).returncode == 0

@@ -202,6 +202,18 @@ def test_emulated_idiv_restoration_matches_oracle(emu, tmp_path, oracle_lib, cas
         assert rel_l2(got, ref64) <= max(2e-6, 4 * rel_l2(ref32, ref64))
 
 
+@pytest.mark.parametrize("case", ["small_even", "small_odd"])
+def test_emulated_correlation_opt_ins_match_oracle(emu, tmp_path, oracle_lib, case):
+    # the conjugated OTF in the z pass: correlation, and RL whose second
+    # convolution is the correlation
+    d = load_golden(case)
+    img, psf = d["image"], d["psf"]
+    assert rel_l2(run_emu(emu, tmp_path, "correlate", img, psf, 0),
+                  oracle_lib.correlate(img, psf)) <= 1e-6
+    assert rel_l2(run_emu(emu, tmp_path, "rlcorr", img, psf, 3),
+                  oracle_lib.rl_correlate(img, psf, 3)) <= 2e-6
+
+
 def test_emulated_idiv_restoration_zero_iterations_returns_the_image(emu, tmp_path):
     # no step taken: s = (sqrt g)^2 on the image region, non-negative
     d = load_golden("small_even")

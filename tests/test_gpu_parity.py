@@ -390,3 +390,22 @@ def test_idiv_restoration_vs_oracle(clarity_gpu, oracle_lib, case, alpha):
         got = out.cpu().numpy()
         assert np.all(got >= 0)
         assert rel_l2(got, ref64) <= max(1e-5, 4 * rel_l2(ref32, ref64))
+
+
+@pytest.mark.parametrize("case", ["small_even", "small_odd", "cfg0_rl10"])
+def test_correlation_opt_ins_vs_oracle(clarity_gpu, oracle_lib, case):
+    # the conjugate-for-correlation opt-ins (conjugated OTF in the z pass)
+    # against the oracle's restatement; the reference forms are unchanged
+    import torch
+    d = load_golden(case)
+    img, psf = d["image"], d["psf"]
+    di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
+    out = torch.empty_like(di)
+    clarity_gpu.correlate_device(di, dk, out)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), oracle_lib.correlate(img, psf)) <= TOL_ONE
+    clarity_gpu.ml_correlate_device(di, dk, out, 4)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), oracle_lib.rl_correlate(img, psf, 4)) <= TOL_ITER
+    plain = clarity_gpu.maximum_likelihood_deconvolve(img, psf, 4)
+    assert rel_l2(plain, oracle_lib.rl(img, psf, 4)) <= TOL_ITER
