@@ -319,6 +319,58 @@ def _cfg2_case(i):
     return img, psf
 
 
+def cached_reference(name, inputs):
+    """A full-size CPU reference the GPU parity tests keep under
+    tests/golden/_large (same key: the name and a digest of the inputs), or
+    None when it has not been computed."""
+    import hashlib
+    h = hashlib.sha1()
+    for a in inputs:
+        h.update(np.ascontiguousarray(a).tobytes())
+    path = os.path.join(ROOT, "tests", "golden", "_large", f"{name}-{h.hexdigest()[:16]}.npy")
+    return np.load(path) if os.path.exists(path) else None
+
+
+def precision_forms(api, torch, stream, iters=100):
+    """The precision workload: RL for `iters` iterations on the 512x512x128
+    volume (work box 1024x1024x256) with the FP32 register FFT and with the
+    first radix-16 z stage as split hi+lo FP16 / BF16 tensor-core GEMMs; time
+    (CUDA events) and the error against the FP64 oracle where its output has
+    been computed (tests/golden/_large)."""
+    from clarity_b200 import synthetic as syn
+    img, psf, _ = syn.cfg3()
+    r64 = cached_reference(f"rl{iters}-f64", [img, psf])
+    r32 = cached_reference(f"rl{iters}-ref32", [img, psf])
+    di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
+    out = torch.empty_like(di)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {"workload": f"RL 512x512x128 fp32 (work box 1024x1024x256), {iters} iterations",
+           "fp64_reference": r64 is not None}
+    if r64 is not None and r32 is not None:
+        res["reference_build_rel_l2_vs_fp64"] = float(np.linalg.norm(
+            (r32.astype(np.float64) - r64).ravel()) / np.linalg.norm(r64.ravel()))
+    for mode, name in ((0, "f32_simt"), (1, "f16_split_tc"), (2, "bf16_split_tc")):
+        api.set_dft_precision(mode)
+        try:
+            api.ml_device(di, dk, out, 1, stream)  # warm-up
+            torch.cuda.synchronize()
+            e0.record(stream)
+            api.ml_device(di, dk, out, iters, stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        finally:
+            api.set_dft_precision(0)
+        ms = e0.elapsed_time(e1)
+        row = {"ms": ms, "value": img.size * iters / (ms / 1e3) / 1e9, "unit": "Gvoxel-iter/s"}
+        if r64 is not None:
+            got = out.cpu().numpy().astype(np.float64)
+            row["rel_l2_vs_fp64"] = float(np.linalg.norm((got - r64).ravel()) /
+                                          np.linalg.norm(r64.ravel()))
+            row["max_abs_vs_fp64"] = float(np.abs(got - r64).max())
+        res[name] = row
+    return res
+
+
 def other_configs(api, torch, stream, n_batch=64, batch_iters=30, cfg3_iters=10):
     """The batched and the large-volume workloads, measured beside the headline
     (G image-voxel-iterations/s; CUDA events on the launching stream)."""
@@ -360,6 +412,8 @@ def other_configs(api, torch, stream, n_batch=64, batch_iters=30, cfg3_iters=10)
                                    "iterations, FP32 SIMT FFT", "ms": ms,
                        "value": img.size * cfg3_iters / (ms / 1e3) / 1e9,
                        "unit": "Gvoxel-iter/s"}
+    del di, dk, out
+    res["precision_forms"] = precision_forms(api, torch, stream)
     return res
 
 

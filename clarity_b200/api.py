@@ -66,7 +66,9 @@ EXTENSION_SYMBOLS = [
     "clarityx_nn_pool2", "clarityx_nn_merge_skip_grad", "clarityx_nn_up_grad",
     "clarityx_nn_adam", "clarityx_nn_pack_weights",
     "clarityx_ml_learned_device", "clarityx_nn_predict", "clarityx_nn_param_count",
+    "clarityx_set_dft_precision", "clarityx_dft_precision",
 ]
+DFT_F32, DFT_F16_SPLIT, DFT_BF16_SPLIT = 0, 1, 2
 BATCH_GRAPH = 1  # CLARITYX_BATCH_GRAPH
 
 
@@ -173,6 +175,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         L.clarityx_nn_predict.argtypes = [vp, C.c_longlong, vp, Dim3, vp, vp]
         L.clarityx_nn_predict.restype = i
         L.clarityx_nn_param_count.restype = C.c_longlong
+        L.clarityx_set_dft_precision.argtypes = [i]
+        L.clarityx_set_dft_precision.restype = i
+        L.clarityx_dft_precision.restype = i
         L.clarityx_autotune.argtypes = [i]
         L.clarityx_autotune.restype = None
         L.clarityx_launch_count.restype = C.c_longlong
@@ -437,6 +442,16 @@ def ml_batch_device(images, kernels, outs, iterations, graph=True, stream=None):
     _check(load().clarityx_ml_batch_device(n, imgs, ids, kers, kds, outp, int(iterations),
                                            BATCH_GRAPH if graph else 0, _stream_ptr(stream)))
     return outs
+
+
+def set_dft_precision(mode: int) -> None:
+    """clarityx_set_dft_precision: 0 FP32 register passes (default), 1 the
+    split hi+lo FP16 tensor-core first z stage, 2 the same in BF16."""
+    _check(load().clarityx_set_dft_precision(int(mode)))
+
+
+def dft_precision() -> int:
+    return int(load().clarityx_dft_precision())
 
 
 def autotune(on: bool = True) -> None:

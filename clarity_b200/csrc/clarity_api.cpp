@@ -724,6 +724,14 @@ ClarityResult_t clarityx_ml_batch_device(int count, const float* const* images,
   return report(s);
 }
 
+ClarityResult_t clarityx_set_dft_precision(int mode) {
+  if (mode < 0 || mode > 2) return fail(CLARITY_INVALID_ARGUMENT, "DFT precision mode must be 0, 1 or 2");
+  clarity::set_dft_precision(mode);
+  return CLARITY_SUCCESS;
+}
+
+int clarityx_dft_precision(void) { return clarity::dft_precision(); }
+
 void clarityx_autotune(int on) {
   std::lock_guard<std::mutex> lk(g_mu);
   g_autotune = on != 0;

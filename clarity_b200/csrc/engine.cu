@@ -124,6 +124,10 @@ int static_family_mask() {
 
 static inline void count_small() { g_launches.fetch_add(1); }
 
+static std::atomic<int> g_dft_precision{0};
+void set_dft_precision(int mode) { g_dft_precision.store(mode); }
+int dft_precision() { return g_dft_precision.load(); }
+
 cudaError_t smem_opt_in(const void* kernel, int smem) {
   if (smem <= 48 * 1024) return cudaSuccess;
   static std::mutex mu;
@@ -549,7 +553,10 @@ static void free_entry(PlanEntry& pe) {
 }
 
 Status Context::plan(const Dims& wd, const PlanEntry** out) {
-  auto key = std::make_tuple(wd.x, wd.y, wd.z);
+  // tuned and default plans are cached apart: a plan the autotuner picked
+  // (by timings that vary from run to run) must not serve calls made with
+  // autotuning off, or results would depend on what ran before
+  auto key = std::make_tuple(wd.x, wd.y, wd.z, autotune_ ? 1 : 0);
   auto it = plans_.find(key);
   if (it != plans_.end()) {
     *out = it->second.get();

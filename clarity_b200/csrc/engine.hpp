@@ -125,7 +125,8 @@ class Context {
   bool has_user_stream_ = false;
   Status build_entry(const VolPlan& P, std::unique_ptr<PlanEntry>* out);
   Status tune(const Dims& wd, std::unique_ptr<PlanEntry>* out);
-  std::map<std::tuple<int, int, int>, std::unique_ptr<PlanEntry>> plans_;
+  // keyed by the work box and whether the autotuner chose the plan
+  std::map<std::tuple<int, int, int, int>, std::unique_ptr<PlanEntry>> plans_;
   Workspace ws_;
   std::vector<std::unique_ptr<Workspace>> slots_;
   std::vector<cudaStream_t> bstreams_;
@@ -222,6 +223,11 @@ bool pdl_enabled();
 cudaError_t smem_opt_in(const void* kernel, int smem);
 long long launch_count();
 int static_family_mask();
+// DFT precision mode of the specialised z pass (0 FP32 register passes, 1
+// split hi+lo FP16 tensor-core first z stage, 2 the same in BF16); applies
+// to shapes with a 16 x 16 z axis (the 1024 x 1024 x 256 box).
+void set_dft_precision(int mode);
+int dft_precision();
 void timing_enable(bool on);
 // Synchronises the recorded events and returns per-kind totals (ms) and
 // counts; clears the record.

@@ -10,6 +10,7 @@
 #include "dft_codelets.cuh"
 #include "launch_macro.cuh"
 #include "plan.hpp"
+#include "tc_dft.cuh"
 #include "tma.cuh"
 
 // Blocks per SM the XY kernels' register budget is sized for (a build
@@ -613,7 +614,26 @@ __global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
   mid.finish();
 }
 
-template <class SH, class Mod>
+// First z stage of the spectral pass: the FP32 register pass, or (PREC > 0,
+// a 16 x 16 z axis) its tensor-core form on split hi+lo operands.
+template <class SH, int DIR, int PREC>
+__device__ __forceinline__ void z_stage0(float2* sm, const float2* __restrict__ tw) {
+#ifndef CLARITY_HOST_EMULATION
+  if constexpr (PREC != kDftF32) {
+    z_stage16_tc<SH, DIR, PREC>(sm, tw);
+    return;
+  }
+#endif
+  z_tile_pass<SH, typename SH::Z, 0, DIR, true>(sm, tw);
+}
+
+// Whether the tensor-core z stage applies to a shape: radix 16 first, whole
+// groups of 8 lines, the tiled (not per-line) z kernel.
+template <class SH>
+constexpr bool kTcZ = SH::Z::radix(0) == 16 && SH::Z::npass >= 2 && SH::BW % 8 == 0 &&
+                      !SH::Y_PER_LINE;
+
+template <class SH, class Mod, int PREC = kDftF32>
 __global__ void __launch_bounds__(256, 2)
     ks_z(const Mod mod, const float2* __restrict__ Sin, float2* __restrict__ Sout,
          const Tables T) {
@@ -640,7 +660,7 @@ __global__ void __launch_bounds__(256, 2)
   } else {
     // all z passes but the last, then last + spectral op + first inverse
     if constexpr (SH::Z::npass >= 2) {
-      z_tile_pass<SH, typename SH::Z, 0, -1, true>(sm, T.twz);
+      z_stage0<SH, -1, PREC>(sm, T.twz);
       __syncthreads();
     }
     if constexpr (SH::Z::npass >= 3) {
@@ -654,7 +674,7 @@ __global__ void __launch_bounds__(256, 2)
       __syncthreads();
     }
     if constexpr (SH::Z::npass >= 2) {
-      z_tile_pass<SH, typename SH::Z, 0, +1, true>(sm, T.twz);
+      z_stage0<SH, +1, PREC>(sm, T.twz);
       __syncthreads();
     }
     tile_inverse_down_to<SH, typename SH::Y, 0, false>(sm, T.twy);

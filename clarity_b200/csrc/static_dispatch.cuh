@@ -130,6 +130,12 @@ inline bool try_static(const PlanEntry& pe, cudaStream_t st, const F& fn, float2
       note_launch_end(KK_Z, st);
     } else {
       auto k = st::ks_z<SH, F>;
+      if constexpr (st::kTcZ<SH> && !F::forward_only) {
+        // the precision form: tensor-core first z stage (the OTF stays FP32)
+        const int prec = dft_precision();
+        if (prec == st::kDftF16Split) k = st::ks_z<SH, F, st::kDftF16Split>;
+        if (prec == st::kDftBF16Split) k = st::ks_z<SH, F, st::kDftBF16Split>;
+      }
       *err = allow_smem_st(k, SH::Z_SMEM);
       if (*err != cudaSuccess) return true;
       note_launch_begin(KK_Z, st);

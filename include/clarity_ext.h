@@ -159,6 +159,19 @@ CLARITY_API ClarityResult_t clarityx_ml_batch_device(
  * passes each) and keeps the fastest. */
 CLARITY_API void clarityx_autotune(int on);
 
+/* Precision form of the 3-D FFT (no reference counterpart; the reference
+ * calls FFTW/cuFFT in FP32).  0 (default): every DFT stage in FP32 register
+ * passes.  1: the first radix-16 stage of the z axis (forward and inverse)
+ * as tensor-core GEMMs on split hi+lo FP16 operands with FP32 accumulation,
+ * each 8-line tile scaled by a power of two into FP16's range -- FP32-class
+ * accuracy.  2: the same on split hi+lo BF16 operands (no scaling, about
+ * 2^-16 relative per stage).  It applies to work boxes whose specialised z
+ * pass has a 16 x 16 z axis (the 1024 x 1024 x 256 box of a 512 x 512 x 128
+ * image with a same-size kernel); other boxes, and every OTF, stay FP32.
+ * Process-wide; returns CLARITY_INVALID_ARGUMENT for other modes. */
+CLARITY_API ClarityResult_t clarityx_set_dft_precision(int mode);
+CLARITY_API int clarityx_dft_precision(void);
+
 CLARITY_API ClarityResult_t clarityx_blind_ml_device(
     const float *image, Clarity_Dim3 imageDim, const float *kernel,
     Clarity_Dim3 kernelDim, float *out, int iterations, void *stream);

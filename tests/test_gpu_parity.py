@@ -227,12 +227,17 @@ def test_batch_argument_errors(clarity_gpu):
 def test_autotuned_plan_matches_oracle(clarity_gpu, oracle_lib):
     # the autotuner may pick any candidate tiling: results stay within parity
     img, psf = _batch_inputs(12, [(12, 40, 36)])
+    before = clarity_gpu.maximum_likelihood_deconvolve(img[0], psf[0], 3)
     clarity_gpu.autotune(True)
     try:
         out = clarity_gpu.maximum_likelihood_deconvolve(img[0], psf[0], 3)
     finally:
         clarity_gpu.autotune(False)
     assert rel_l2(out, oracle_lib.rl(img[0], psf[0], 3)) <= TOL_ITER
+    # with autotuning off again the default plan serves the box, so results
+    # do not depend on whether (or how) the tuner ran before
+    after = clarity_gpu.maximum_likelihood_deconvolve(img[0], psf[0], 3)
+    assert np.array_equal(before, after)
 
 
 @pytest.mark.parametrize("case", ["small_even", "cfg0_rl10"])
@@ -328,13 +333,9 @@ def test_u16_raw_path_and_app(clarity_gpu, tmp_path):
                         "36", "40", "12", str(tmp_path / "out.raw")], capture_output=True, text=True)
     assert p.returncode == 0, p.stdout + p.stderr
     app = np.fromfile(tmp_path / "out.raw", np.uint16).reshape(img.shape)
-    # another process may round the float result differently in the last
-    # bits (within the float path's tolerance); truncation then moves a value
-    # by one only where that result lies next to an integer
-    diff = app.astype(np.int64) - got.astype(np.int64)
-    assert np.abs(diff).max() <= 1
-    near = np.abs(ref - np.round(ref)) <= 1e-5 * np.maximum(1.0, np.abs(ref))
-    assert np.all(near[diff != 0])
+    # the same plan in every process (autotuned plans are cached apart from
+    # the default ones): the app's result is bit-identical
+    assert np.array_equal(app, got)
 
 
 # (case, outer iterations, PSF sub-steps).  With the PSF spanning the whole
