@@ -264,7 +264,7 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
         net = learned.load_net()
         for tag, accel in (("learned_start", False), ("learned_start_accel", True)):
             k_ls, ls_final = None, None
-            for k in range(1, max_accel + 1):
+            for k in range(0, max_accel + 1):
                 tl = torch.zeros(k + 1, dtype=torch.float64, device="cuda")
                 learned.learned_solve(net, img_d, psf_d, out, k, idiv=tl, stream=stream,
                                       accel=accel)

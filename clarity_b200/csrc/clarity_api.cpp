@@ -139,6 +139,8 @@ cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t st) 
   return cudaSuccess;
 }
 
+bool g_implicit = false;         // the context was created by a call, not by Register
+
 void set_error(const char* msg) {
   std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg ? msg : "");
 }
@@ -179,6 +181,50 @@ void free_staging() {
   free_bounce();
 }
 
+// Creates the library context on the selected device (g_mu held).
+ClarityResult_t create_context_locked(const char* who) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count <= g_device)
+    return fail(CLARITY_INVALID_OPERATION, std::string(who) + ": no CUDA device available");
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, g_device);
+  if (e != cudaSuccess)
+    return fail(CLARITY_INVALID_OPERATION, std::string(who) + ": " + cudaGetErrorString(e));
+  if (prop.major != 10)
+    return fail(CLARITY_INVALID_OPERATION,
+                std::string(who) + ": device is not sm_100 class: " + prop.name);
+  Context* c = new Context(g_device);
+  const Status is = c->init();
+  if (!is.ok()) {
+    delete c;
+    return report(is);
+  }
+  c->set_autotune(g_autotune);
+  g_ctx = c;
+  if (std::getenv("CLARITY_LOG"))
+    std::fprintf(stderr, "clarity: device %d '%s', %zu MB\n", g_device, prop.name,
+                 (size_t)(prop.totalGlobalMem >> 20));
+  return CLARITY_SUCCESS;
+}
+
+// The context a call runs on.  Callers of the reference need not call
+// Clarity_Register first -- its functions work without it, and its own
+// raw-image app (apps/DeconvolveRawImages/DeconvolveRawImages.cxx) never
+// calls it -- so the first call without a registration creates the context
+// itself.  A later Clarity_Register adopts it; Clarity_UnRegister releases it
+// when the registrations balance, and otherwise it lives until the process
+// exits.
+Context* acquire_context(ClarityResult_t* rc) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_ctx) {
+    *rc = create_context_locked("Clarity_Register (implicit, on first use)");
+    if (*rc != CLARITY_SUCCESS) return nullptr;
+    g_implicit = true;
+  }
+  return g_ctx;
+}
+
 // Common path of the host-buffer algorithms: validate, upload, run, download.
 template <class Run>
 ClarityResult_t host_call(const float* in, Clarity_Dim3 id, const float* ker,
@@ -186,12 +232,9 @@ ClarityResult_t host_call(const float* in, Clarity_Dim3 id, const float* ker,
   if (!in || !ker || !out) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
   if (!dims_ok(id) || !dims_ok(kd))
     return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
-  Context* ctx;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    ctx = g_ctx;
-  }
-  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  ClarityResult_t rc_ = CLARITY_SUCCESS;
+  Context* ctx = acquire_context(&rc_);
+  if (!ctx) return rc_;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   ctx->clear_stream();
@@ -222,12 +265,9 @@ ClarityResult_t device_call(const float* in, Clarity_Dim3 id, const float* ker,
   if (!in || !ker || !out) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
   if (!dims_ok(id) || !dims_ok(kd))
     return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
-  Context* ctx;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    ctx = g_ctx;
-  }
-  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  ClarityResult_t rc_ = CLARITY_SUCCESS;
+  Context* ctx = acquire_context(&rc_);
+  if (!ctx) return rc_;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   // a bounded wait of earlier work that gave up is reported here (that
@@ -264,27 +304,12 @@ Clarity_Dim3 Clarity_Dim3FromArray(int dimArray[3]) {
 ClarityResult_t Clarity_Register(void) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (g_refcount == 0) {
-    int count = 0;
-    cudaError_t e = cudaGetDeviceCount(&count);
-    if (e != cudaSuccess || count <= g_device)
-      return fail(CLARITY_INVALID_OPERATION, "no CUDA device available");
-    cudaDeviceProp prop;
-    e = cudaGetDeviceProperties(&prop, g_device);
-    if (e != cudaSuccess) return fail(CLARITY_INVALID_OPERATION, cudaGetErrorString(e));
-    if (prop.major != 10)
-      return fail(CLARITY_INVALID_OPERATION,
-                  std::string("device is not sm_100 class: ") + prop.name);
-    g_ctx = new Context(g_device);
-    const Status is = g_ctx->init();
-    if (!is.ok()) {
-      delete g_ctx;
-      g_ctx = nullptr;
-      return report(is);
+    if (g_ctx) {
+      g_implicit = false;  // adopt the context an earlier call created
+    } else {
+      const ClarityResult_t r = create_context_locked("Clarity_Register");
+      if (r != CLARITY_SUCCESS) return r;
     }
-    g_ctx->set_autotune(g_autotune);
-    if (std::getenv("CLARITY_LOG"))
-      std::fprintf(stderr, "clarity: device %d '%s', %zu MB\n", g_device, prop.name,
-                   (size_t)(prop.totalGlobalMem >> 20));
   }
   g_refcount++;
   return CLARITY_SUCCESS;
@@ -458,7 +483,8 @@ const char* clarityx_last_error(void) { return g_last_error; }
 
 ClarityResult_t clarityx_set_device(int device) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (g_refcount > 0) return fail(CLARITY_INVALID_OPERATION, "already registered");
+  if (g_refcount > 0 || g_ctx)
+    return fail(CLARITY_INVALID_OPERATION, "already registered (or a call created the context)");
   if (device < 0) return fail(CLARITY_INVALID_ARGUMENT, "negative device");
   g_device = device;
   return CLARITY_SUCCESS;
@@ -580,12 +606,9 @@ ClarityResult_t clarityx_nn_predict(const float* params, long long nparams, cons
   if (!dims_ok(dim)) return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
   if (nparams != clarity::nn_param_count())
     return fail(CLARITY_INVALID_ARGUMENT, "network parameters: wrong count");
-  Context* ctx;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    ctx = g_ctx;
-  }
-  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  ClarityResult_t rc_ = CLARITY_SUCCESS;
+  Context* ctx = acquire_context(&rc_);
+  if (!ctx) return rc_;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   Status s = ctx->check_device_errors();
@@ -628,12 +651,9 @@ ClarityResult_t clarityx_ml_u16(const uint16_t* image, Clarity_Dim3 imageDim,
   if (!image || !kernel || !out) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
   if (!dims_ok(imageDim) || !dims_ok(kernelDim))
     return fail(CLARITY_INVALID_ARGUMENT, "dimension <= 0");
-  Context* ctx;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    ctx = g_ctx;
-  }
-  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  ClarityResult_t rc_ = CLARITY_SUCCESS;
+  Context* ctx = acquire_context(&rc_);
+  if (!ctx) return rc_;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   ctx->clear_stream();
@@ -707,12 +727,9 @@ ClarityResult_t clarityx_ml_batch_device(int count, const float* const* images,
     ids[i] = to_dims(imageDims[i]);
     kds[i] = to_dims(kernelDims[i]);
   }
-  Context* ctx;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    ctx = g_ctx;
-  }
-  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  ClarityResult_t rc_ = CLARITY_SUCCESS;
+  Context* ctx = acquire_context(&rc_);
+  if (!ctx) return rc_;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   Status s = ctx->check_device_errors();
@@ -766,8 +783,9 @@ ClarityResult_t clarityx_idivergence(const float* g, const float* ghat, long lon
                                      double* result) {
   if (!g || !ghat || !result) return fail(CLARITY_INVALID_ARGUMENT, "NULL buffer");
   if (n <= 0) return fail(CLARITY_INVALID_ARGUMENT, "n <= 0");
-  Context* ctx = g_ctx;
-  if (!ctx) return fail(CLARITY_INVALID_OPERATION, "Clarity_Register has not been called");
+  ClarityResult_t rc_ = CLARITY_SUCCESS;
+  Context* ctx = acquire_context(&rc_);
+  if (!ctx) return rc_;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device());
   ctx->clear_stream();

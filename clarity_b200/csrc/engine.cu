@@ -1069,10 +1069,26 @@ static Status rl_solve(Context& ctx, const PlanEntry& pe, Workspace& ws, const f
                        bool correlate = false) {
   cudaStream_t st = ctx.exec_stream();
   if (iters <= 0) {
-    // the reference leaves the output unwritten; return the input image
+    // no iteration: the estimate RL would start from (the reference leaves
+    // the output unwritten; here the input image, or `start`)
+    const float* est = start ? start : img;
     count_small();
-    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, st)(img, out, id.n());
+    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, st)(est, out, id.n());
     CL_CHECK(cudaGetLastError());
+    if (idiv) {
+      // idiv[0]: that estimate's own I-divergence (one convolution)
+      const VolPlan& P = pe.P;
+      CL_TRY(make_otf(ctx, pe, ker, kd, wd, ws.H, nullptr));
+      CL_TRY(xy_forward(ctx, pe, ProImage{image_src(est, id), P.xmode}, ws.S));
+      CL_TRY(z_pass(ctx, pe, ModOTF{ws.H, inv_volume(wd)}, ws.S, ws.S));
+      MidRLRatio tr{image_src(img, id), P.xmode};
+      tr.idiv_partial = ws.partial;
+      tr.nblocks = ws.iscal + 1;
+      CL_TRY(xy_inverse(ctx, pe, tr, ws.S));
+      count_small();
+      CLARITY_LAUNCH(k_finish_sum_np, 1, 256, 0, st)(ws.partial, ws.iscal + 1, idiv);
+      CL_CHECK(cudaGetLastError());
+    }
     return Status::Ok();
   }
   CL_TRY(make_otf(ctx, pe, ker, kd, wd, ws.H, nullptr));
@@ -1128,12 +1144,6 @@ Status run_rl_ex(Context& ctx, const float* img, Dims id, const float* ker, Dims
   Workspace* ws;
   Dims wd;
   CL_TRY(setup(ctx, id, kd, &pe, &ws, &wd));
-  if (iters <= 0 && start) {
-    count_small();
-    CLARITY_LAUNCH(k_copy, kReduceBlocks, 256, 0, ctx.exec_stream())(start, out, id.n());
-    CL_CHECK(cudaGetLastError());
-    return Status::Ok();
-  }
   return rl_solve(ctx, *pe, *ws, img, id, ker, kd, wd, out, iters, start, idiv);
 }
 

@@ -32,7 +32,7 @@ typedef enum {
   CLARITY_FFT_FAILED = 0,           /* an FFT stage could not run          */
   CLARITY_OUT_OF_MEMORY = 1,        /* host allocation failed              */
   CLARITY_DEVICE_OUT_OF_MEMORY = 2, /* device allocation failed            */
-  CLARITY_INVALID_OPERATION = 3,    /* not registered, or a device failure */
+  CLARITY_INVALID_OPERATION = 3,    /* no usable device, or a device failure */
   CLARITY_INVALID_ARGUMENT = 4,     /* NULL pointer or dimension <= 0      */
   CLARITY_SUCCESS = 5
 } ClarityResult_t;
@@ -51,7 +51,10 @@ CLARITY_API Clarity_Dim3 Clarity_Dim3FromArray(int dimArray[3]);
 /* Reference-counted initialisation (Clarity.h.in:137-139;
  * src/Clarity.cxx:46-79).  The first call selects the CUDA device and
  * creates the library context; later calls only bump the count.  Returns
- * CLARITY_INVALID_OPERATION when no usable sm_100 device is present. */
+ * CLARITY_INVALID_OPERATION when no usable sm_100 device is present.
+ * As with the reference, calling it is optional: a call made without a
+ * registration creates the context itself (the reference's own raw-image
+ * app never registers), and a later Clarity_Register adopts that context. */
 CLARITY_API ClarityResult_t Clarity_Register(void);
 
 /* Clarity.h.in:147-149; src/Clarity.cxx:82-91.  The last call releases

@@ -231,7 +231,7 @@ void rl(const S* in, Dim3 id, const S* kernel, Dim3 kd, S* out, int iters,
     const T scale = energy / ne;
     for (long i = 0; i < n; i++) u[i] = scale * u[i];
   }
-  if (idiv && iters > 0) {  // the result's own I-divergence
+  if (idiv) {  // the result's own I-divergence (the start's, without iterations)
     convolve_otf<T>(w, u.data(), otf.data(), s1.data(), tmp);
     idiv[iters] = idiv_image(w, id, s1.data());
   }
