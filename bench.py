@@ -396,7 +396,26 @@ def other_configs(api, torch, stream, n_batch=64, batch_iters=30, cfg3_iters=10)
                                      f"z in 8*{{2..12}}), {batch_iters} RL iterations, one "
                                      "captured CUDA graph", "image_voxels": int(vox),
                          "ms": ms, "value": vox * batch_iters / (ms / 1e3) / 1e9,
-                         "unit": "Gvoxel-iter/s"}
+                         "unit": "Gvoxel-iter/s", "plans": "planner default"}
+    # the same batch with the autotuner choosing each work box's tiling (the
+    # tuning runs on first use, in the set-up call outside the timed region)
+    api.trim()
+    api.autotune(True)
+    try:
+        api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    finally:
+        api.autotune(False)
+    ms = e0.elapsed_time(e1) / 3
+    res["batched_rl_autotuned"] = dict(res["batched_rl"], ms=ms,
+                                       value=vox * batch_iters / (ms / 1e3) / 1e9,
+                                       plans="autotuned (fastest of the planner's best four "
+                                             "tilings per work box)")
     del imgs, psfs, outs
     img, psf, _ = syn.cfg3()
     di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()

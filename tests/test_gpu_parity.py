@@ -340,10 +340,14 @@ def test_u16_raw_path_and_app(clarity_gpu, tmp_path):
                         "36", "40", "12", str(tmp_path / "out.raw")], capture_output=True, text=True)
     assert p.returncode == 0, p.stdout + p.stderr
     app = np.fromfile(tmp_path / "out.raw", np.uint16).reshape(img.shape)
-    # the same plan in every process (autotuned plans are cached apart from
-    # the default ones): the app's result is bit-identical
-    d = np.abs(app.astype(np.int64) - got.astype(np.int64))
-    assert np.array_equal(app, got), f"{np.count_nonzero(d)} voxels differ, max {d.max()}"
+    # another process may round the float result differently in the last
+    # bit (the work box's generic kernels give one of two results per
+    # process, both equally close to FP64); truncation then moves a value by
+    # one only where that result lies next to an integer
+    diff = app.astype(np.int64) - got.astype(np.int64)
+    assert np.abs(diff).max() <= 1, f"{np.count_nonzero(diff)} voxels differ"
+    near = np.abs(ref - np.round(ref)) <= 1e-5 * np.maximum(1.0, np.abs(ref))
+    assert np.all(near[diff != 0])
 
 
 # (case, outer iterations, PSF sub-steps).  With the PSF spanning the whole
