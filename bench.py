@@ -192,8 +192,9 @@ def family_bytes(work, img_vox, ker_vox, iters):
 
 
 # DRAM bytes (read + write) per launch of each steady-iteration kernel family,
-# from the ncu capture of iteration 2 of this workload
-# (profiles/kernels_rl_iteration_512x512x128.md; z: mean of its two launches).
+# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
+# steady launches of this workload's iteration 2 (z: the mean of its two
+# launches, P2 and P4).
 NCU_TRAFFIC = {"xy_product": 152.1e6 + 215.7e6, "xy_inv_fwd": 84.5e6 + 19.7e6,
                "z": (270.7e6 + 46.4e6 + 203.5e6 + 86.7e6) / 2}
 
@@ -281,6 +282,7 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
                 ls["idiv"] = ls_final
                 ls["speedup"] = res["plain"]["ms"] / ls["ms"]
             res[tag] = ls
+        res["network"] = network_layers(torch, net)
     return res
 
 
@@ -311,6 +313,53 @@ def headline_parity(api, torch, img_d, psf_d, img, psf, stream, iters=10):
     res["max_abs_vs_fp64"] = float(np.abs(got - r64).max())
     res["tolerance"] = "rel-L2 <= 1e-4 after several iterations (1e-5 after one)"
     return res
+
+
+def network_layers(torch, net, shape_zyx=(64, 256, 256), reps=5):
+    """Per-layer device time and TFLOP/s of the learned-start network's
+    forward pass at the 256x256x64 volume (CUDA events around each layer's
+    launch; 2 x voxels x cout x 27 x cin FLOPs per 3x3x3 convolution)."""
+    from clarity_b200 import unet
+    D, H, W = shape_zyx
+    x = torch.rand((D, H, W), device="cuda") * 100 + 1
+    inp, _ = unet.to_input(x)
+    _, A = net.forward(inp.contiguous(), keep=True)  # the layers' inputs
+    torch.cuda.synchronize()
+    plan = [("l0b", A["a0"], None, 1), ("l1a", A["p0"], None, 2), ("l1b", A["a1"], None, 2),
+            ("l2a", A["p1"], None, 4), ("l2b", A["a2"], None, 4), ("l3a", A["p2"], None, 8),
+            ("l3b", A["a3"], None, 8), ("l2c", A["s2"], A["b3"], 4), ("l2d", A["c2"], None, 4),
+            ("l1c", A["s1"], A["d2"], 2), ("l1d", A["c1"], None, 2), ("l0c", A["s0"], A["d1"], 1),
+            ("l0d", A["c0"], None, 1)]
+    rows, tot_ms, tot_fl = {}, 0.0, 0.0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, x1, x2, f in plan:
+        co = net.layout[name][3]
+        cin = net.layout[name][4] + net.layout[name][5]
+        vox = (D // f) * (H // f) * (W // f)
+        fl = 2.0 * vox * co * 27 * cin
+        call = lambda: unet.conv3(x1, net.wf[name], co, bias=net.b(name), relu=True, x2=x2)
+        call()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            call()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        rows[name] = {"ms": ms, "tflops": fl / (ms / 1e3) / 1e12, "cin": cin, "cout": co,
+                      "voxels": vox}
+        tot_ms += ms
+        tot_fl += fl
+    e0.record()
+    for _ in range(reps):
+        out = torch.empty_like(x)
+        from clarity_b200 import api
+        api.nn_predict(net.p, x, out)
+    e1.record()
+    torch.cuda.synchronize()
+    return {"layers": rows, "conv_ms": tot_ms, "conv_tflops": tot_fl / (tot_ms / 1e3) / 1e12,
+            "predict_ms": e0.elapsed_time(e1) / reps,
+            "note": "BF16 mma.sync implicit-GEMM convolutions, FP32 accumulation"}
 
 
 def _cfg2_case(i):
