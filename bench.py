@@ -195,8 +195,8 @@ def family_bytes(work, img_vox, ker_vox, iters):
 # measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
 # steady launches of this workload's iteration 2 (z: the mean of its two
 # launches, P2 and P4).
-NCU_TRAFFIC = {"xy_product": 152.1e6 + 215.7e6, "xy_inv_fwd": 84.5e6 + 19.7e6,
-               "z": (270.7e6 + 46.4e6 + 203.5e6 + 86.7e6) / 2}
+NCU_TRAFFIC = {"xy_product": 152.1e6 + 215.7e6, "xy_inv_fwd": 84.5e6 + 20.9e6,
+               "z": (270.7e6 + 46.0e6 + 203.5e6 + 82.6e6) / 2}
 
 
 def max_over_ranks(value, dist, device):
@@ -265,7 +265,9 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
         net = learned.load_net()
         for tag, accel in (("learned_start", False), ("learned_start_accel", True)):
             k_ls, ls_final = None, None
-            for k in range(0, max_accel + 1):
+            # zero resumed iterations is the prediction itself (the plain form
+            # traces it; the accelerated form starts at one iteration)
+            for k in range(1 if accel else 0, max_accel + 1):
                 tl = torch.zeros(k + 1, dtype=torch.float64, device="cuda")
                 learned.learned_solve(net, img_d, psf_d, out, k, idiv=tl, stream=stream,
                                       accel=accel)
@@ -276,7 +278,7 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
             ls = {"form": f"learned start (3-D U-Net on RL iterate {net.pre}, BF16 tensor-core "
                           "kernels) " + ("+ accelerated RL" if accel else "+ resumed RL"),
                   "pre_iterations": net.pre, "resumed_iterations": k_ls}
-            if k_ls:
+            if k_ls is not None:
                 ls["ms"] = ev_ms(lambda: learned.learned_solve(net, img_d, psf_d, out, k_ls,
                                                                stream=stream, accel=accel))
                 ls["idiv"] = ls_final
