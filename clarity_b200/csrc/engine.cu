@@ -154,8 +154,7 @@ bool xy_tma_enabled() {
 #ifndef CLARITY_HOST_EMULATION
 // cuTensorMapEncodeTiled, fetched from the driver through the runtime (no
 // link-time dependency on libcuda).
-bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
-                          const unsigned long long stride_bytes[3], const unsigned box[4]) {
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -165,15 +164,31 @@ bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long l
       fn = nullptr;
     return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }();
+  return encode;
+}
+static bool encode_4d(TensorMap* tm, CUtensorMapDataType type, const void* base,
+                      const unsigned long long dim[4], const unsigned long long stride_bytes[3],
+                      const unsigned box[4], CUtensorMapSwizzle swizzle) {
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (!encode || ((uintptr_t)base & 15u) != 0) return false;
   const cuuint64_t gdim[4] = {dim[0], dim[1], dim[2], dim[3]};
   const cuuint64_t gstr[3] = {stride_bytes[0], stride_bytes[1], stride_bytes[2]};
   const cuuint32_t bdim[4] = {box[0], box[1], box[2], box[3]};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), gdim, gstr,
-                bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+  return encode(tm, type, 4, const_cast<void*>(base), gdim, gstr, bdim, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
+                          const unsigned long long stride_bytes[3], const unsigned box[4]) {
+  return encode_4d(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, base, dim, stride_bytes, box,
+                   CU_TENSOR_MAP_SWIZZLE_NONE);
+}
+bool encode_tensor_bf16_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
+                           const unsigned long long stride_bytes[3], const unsigned box[4],
+                           bool swizzle32) {
+  return encode_4d(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, dim, stride_bytes, box,
+                   swizzle32 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE);
 }
 #else
 bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],

@@ -23,6 +23,8 @@
 #include <cuda_bf16.h>
 
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 #include "engine.hpp"
 #include "launch_macro.cuh"
@@ -46,6 +48,7 @@ struct Conv3Args {
   int relu;
   const bf16* mask;  // optional [v][cout]: result *= (mask > 0)
   bf16* y;           // [v][cout]
+  int* err = nullptr;  // error word for bounded waits that give up (tcgen05 path)
 };
 
 constexpr int kBM = 128;   // voxels per block
@@ -269,6 +272,396 @@ __global__ void __launch_bounds__(128) k_conv3(const Conv3Args a) {
   }
 #endif
 }
+
+// ------------------------------------------------- tcgen05 convolution
+// The same convolution on the 5th-generation tensor cores, for volumes whose
+// width is a multiple of 32.  One MMA computes 128 output voxels -- a tile of
+// tx consecutive x voxels by ty = 128 / tx rows (tx = 128, 64 or 32) -- for BN
+// output channels, accumulating in tensor memory (TMEM).  A work item is R
+// such tiles stacked along y in one z plane; a persistent block takes items
+// round-robin.  For each item the reduction runs over units (16-channel
+// chunk, dz): per unit
+//   * the load warp brings, by TMA, the unit's input slab (the plane z + dz - 1,
+//     rows y0 - 1 .. y0 + R ty, columns x0 - 1 .. x0 + tx, 16 channels; zero
+//     outside the volume; for a chunk of the half-resolution input the
+//     matching coarse slab) and the 9 taps' weights of that dz into a stage;
+//   * eight window warps (two per TMEM lane quarter) turn the slab into the A
+//     operands in TMEM: thread m (TMEM lane m = MMA row m) reads its voxel's 16
+//     channels from the slab and its x neighbours arrive by warp shuffles, so
+//     every tap's shifted window (3 x shifts by S start rows) is written once
+//     with tcgen05.st;
+//   * one issuing thread per MMA tile (R of them) issues that tile's 9 MMAs
+//     (A from TMEM, B = the taps' weights from shared memory) and commits them
+//     to the barriers that free the stage and the window buffer.  A single
+//     thread issues one tcgen05.mma about every 46 cycles whatever N is, so
+//     with N = 16 only several issuers keep the tensor cores busy;
+//   * four epilogue warps read a finished item's accumulators (tcgen05.ld),
+//     add bias, apply ReLU or the mask and store BF16, while the MMAs of the
+//     next item run into the other accumulator buffer.
+// Shared memory holds kTmStages stages; TMEM holds two window buffers and one
+// or two accumulator buffers.  Every wait is bounded: a wait that runs out
+// records a timeout in the error word and sets the block's abort flag, the
+// other roles stop at their next wait, in-flight copies and MMAs are waited
+// for (again bounded) and the TMEM is freed.
+#ifndef CLARITY_HOST_EMULATION
+// warps 0-3 epilogue, 4-11 windows (two per TMEM lane quarter), 12 loads,
+// 13-16 MMA issue (one per MMA tile of an item)
+constexpr int kTmWinWarps = 8;
+constexpr int kTmLoadWarp = 4 + kTmWinWarps;
+constexpr int kTmIssueWarp = kTmLoadWarp + 1;
+constexpr int kTmIssuers = 4;
+constexpr int kTmThreads = 32 * (kTmIssueWarp + kTmIssuers);
+constexpr int kTmStages = 4;
+constexpr int kTmCols = 512;     // TMEM columns the block allocates
+constexpr long long kTmWaitLimit = 1ll << 22;  // polls of an mbarrier before giving up
+constexpr unsigned kFull = 0xffffffffu;
+
+struct TmGeom {
+  int tx, ty, R, rows, S;    // MMA tile tx x ty voxels; R tiles per item; S window rows
+  int nxb, nyb, nnb, items;  // items: x blocks x y blocks x z x channel blocks
+  int na;                    // accumulator buffers (1 or 2)
+  int cw1, cw2;              // slab row lengths (voxels) of the full- and half-resolution inputs
+  uint32_t stage, wofs;      // bytes of a stage; offset of its weights
+  uint32_t tx1, tx2;         // bytes a stage receives for a full- / half-resolution chunk
+  uint32_t acc_cols, win_cols;
+};
+
+// Shared-memory matrix descriptor: K-major, no swizzle, 16-byte rows with
+// 8-row core matrices 128 bytes apart (SBO) and the second 8 K-elements
+// lbo bytes away (LBO); version 1 (bits 46-47) as sm_100 requires.
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)(128u >> 4) << 32) | ((uint64_t)1 << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+// D (TMEM) (+)= A (TMEM, 128 lanes x 16 BF16) x B (shared memory descriptor)
+__device__ __forceinline__ void tc_mma_ts(uint32_t d, uint32_t a, uint64_t b, uint32_t id,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      ::"r"(d), "r"(a), "l"(b), "r"(id), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               ::"r"(su32(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tc_st8(uint32_t taddr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
+      ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
+        "r"(v[7])
+      : "memory");
+}
+__device__ __forceinline__ void tc_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tm_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
+}
+// Bounded wait that also gives up when another role of the block has
+// aborted; the role that runs out of polls records the timeout.
+__device__ __forceinline__ bool tm_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                        int* err) {
+  for (long long it = 0; it < kTmWaitLimit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255) == 255 && *abort) return false;
+  }
+  *abort = 1;
+  raise_error(err, kErrWaitTimeout);
+  return false;
+}
+
+// Item -> (z, y0, x0, first output channel)
+struct TmItem {
+  int z, y0, x0, co0;
+};
+__device__ __forceinline__ TmItem tm_item(const TmGeom& g, int item, int bn) {
+  int r = item;
+  const int nb = r % g.nnb;
+  r /= g.nnb;
+  const int xb = r % g.nxb;
+  r /= g.nxb;
+  const int yb = r % g.nyb;
+  return TmItem{r / g.nyb, yb * g.rows, xb * g.tx, nb * bn};
+}
+
+// 16 channels of the slab voxel (hr, hc) (halo coordinates: row 0 = y0 - 1,
+// column 0 = x0 - 1), from the stage's 32-byte-swizzled slab.  For a
+// half-resolution chunk the voxel's coarse parent is read.
+__device__ __forceinline__ void tm_slab(const unsigned char* st, const TmGeom& g, bool full,
+                                        int y0, int x0, int hr, int hc, uint32_t* v) {
+  int off;
+  if (full) {
+    off = (hr * g.cw1 + hc) * 32;
+  } else {
+    const int yr = ((y0 - 1 + hr) >> 1) - ((y0 - 1) >> 1);
+    const int xc = ((x0 - 1 + hc) >> 1) - ((x0 - 1) >> 1);
+    off = (yr * g.cw2 + xc) * 32;
+  }
+  const int sw = (off >> 7) & 1;  // the swizzle exchanges the halves when bit 7 is set
+  const uint4 lo = *reinterpret_cast<const uint4*>(st + off + 16 * sw);
+  const uint4 hi = *reinterpret_cast<const uint4*>(st + off + 16 * (sw ^ 1));
+  v[0] = lo.x; v[1] = lo.y; v[2] = lo.z; v[3] = lo.w;
+  v[4] = hi.x; v[5] = hi.y; v[6] = hi.z; v[7] = hi.w;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kTmThreads, 1)
+    k_conv3_tm(const Conv3Args a, const TmGeom g, CLARITY_GRID_CONST TensorMap m1,
+               CLARITY_GRID_CONST TensorMap m2, CLARITY_GRID_CONST TensorMap mw) {
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 128, "BN: a multiple of 16 up to 128");
+  extern __shared__ unsigned char tm_raw[];
+  unsigned char* base = tm_raw + ((1024u - (su32(tm_raw) & 1023u)) & 1023u);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + kTmStages * g.stage);
+  uint64_t* empty = full + kTmStages;
+  uint64_t* wfull = empty + kTmStages;  // [2] window buffer written
+  uint64_t* wempty = wfull + 2;         // [2] window buffer read by its MMAs
+  uint64_t* afull = wempty + 2;         // [2] accumulators complete
+  uint64_t* aempty = afull + 2;         // [2] accumulators read out
+  uint64_t* drain = aempty + 2;         // [kTmIssuers]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + kTmIssuers);
+  volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nunits = 3 * ((a.c1 + a.c2) / 16);
+  if (warp == kTmLoadWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(su32(tslot)), "r"(kTmCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTmStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kTmWinWarps + g.R);  // window warps + one commit per issuer
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&wfull[b], kTmWinWarps);
+      mbar_init(&wempty[b], g.R);
+      mbar_init(&afull[b], g.R);
+      mbar_init(&aempty[b], 4);
+    }
+    for (int i = 0; i < kTmIssuers; ++i) mbar_init(&drain[i], 1);
+    *abort = 0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t acc0 = tmem, win0 = tmem + (uint32_t)g.na * g.acc_cols;
+
+  if (warp == kTmLoadWarp) {
+    // ---- loads
+    if (lane == 0) {
+      uint32_t q = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x) {
+        const TmItem it = tm_item(g, item, BN);
+        for (int u = 0; u < nunits; ++u, ++q) {
+          const int cc = u / 3, dz = u - 3 * (u / 3);
+          const int s = (int)(q % kTmStages);
+          if (!tm_wait(&empty[s], ((q / kTmStages) & 1) ^ 1, abort, a.err)) {
+            ok = false;
+            break;
+          }
+          unsigned char* st = base + s * g.stage;
+          const bool fullres = cc * 16 < a.c1;
+          mbar_arrive_expect_tx(&full[s], fullres ? g.tx1 : g.tx2);
+          if (fullres)
+            tma_load_4d(st, &m1, cc * 16, it.x0 - 1, it.y0 - 1, it.z + dz - 1, &full[s]);
+          else
+            tma_load_4d(st, &m2, cc * 16 - a.c1, (it.x0 - 1) >> 1, (it.y0 - 1) >> 1,
+                        (it.z + dz - 1) >> 1, &full[s]);
+          tma_load_4d(st + g.wofs, &mw, cc * 16, it.co0, dz * 9, 0, &full[s]);
+          tma_load_4d(st + g.wofs + 9 * BN * 16, &mw, cc * 16 + 8, it.co0, dz * 9, 0, &full[s]);
+        }
+      }
+      // the copies of the last stages have landed before the block exits
+      const uint32_t n = q < (uint32_t)kTmStages ? q : (uint32_t)kTmStages;
+      for (uint32_t k = q - n; k < q; ++k)
+        mbar_wait_bounded(&full[k % kTmStages], (k / kTmStages) & 1, a.err, kTmWaitLimit);
+    }
+    __syncwarp();
+  } else if (warp >= kTmIssueWarp) {
+    // ---- MMA issue: issuer i accumulates MMA tile i of every item
+    const int i = warp - kTmIssueWarp;
+    if (lane == 0 && i < g.R) {
+      constexpr uint32_t kIdesc = tc_idesc(128, BN);
+      uint32_t q = 0, j = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < g.items && ok; item += gridDim.x, ++j) {
+        const uint32_t ab = j % (uint32_t)g.na;
+        if (!tm_wait(&aempty[ab], ((j / g.na) & 1) ^ 1, abort, a.err)) break;
+        tc_fence_after();
+        const uint32_t acc = acc0 + ab * g.acc_cols + (uint32_t)(i * BN);
+        const uint32_t wrow = (uint32_t)(i * g.ty);
+        for (int u = 0; u < nunits; ++u, ++q) {
+          const int s = (int)(q % kTmStages);
+          const uint32_t b = q & 1;
+          if (!tm_wait(&full[s], (q / kTmStages) & 1, abort, a.err) ||
+              !tm_wait(&wfull[b], (q >> 1) & 1, abort, a.err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sw = su32(base + s * g.stage + g.wofs);
+          const uint32_t win = win0 + b * g.win_cols + wrow * 24;
+#pragma unroll
+          for (int t9 = 0; t9 < 9; ++t9) {
+            const int dy = t9 / 3, dx = t9 % 3;
+            tc_mma_ts(acc, win + (uint32_t)((dy * 3 + dx) * 8),
+                      tc_sdesc(sw + (uint32_t)(t9 * BN * 16), 9 * BN * 16), kIdesc,
+                      (u | t9) != 0 ? 1u : 0u);
+          }
+          tc_commit(&wempty[b]);
+          tc_commit(&empty[s]);
+        }
+        if (!ok) break;
+        tc_commit(&afull[ab]);
+      }
+      // every MMA this thread issued has finished before the TMEM is freed
+      tc_commit(&drain[i]);
+      mbar_wait_bounded(&drain[i], 0, a.err, kTmWaitLimit);
+    }
+    __syncwarp();
+  } else if (warp >= 4) {
+    // ---- windows: TMEM lane m = MMA row m = voxel (row m / tx, column m % tx);
+    // two warps per lane quarter take alternate window rows
+    const int quarter = warp & 3, part = (warp - 4) >> 2;
+    const int m = quarter * 32 + lane;
+    const int tr = m / g.tx, tc = m - tr * g.tx;
+    const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    uint32_t q = 0;
+    for (int item = blockIdx.x; item < g.items; item += gridDim.x) {
+      const TmItem it = tm_item(g, item, BN);
+      bool ok = true;
+      for (int u = 0; u < nunits; ++u, ++q) {
+        const int cc = u / 3;
+        const int s = (int)(q % kTmStages);
+        const uint32_t b = q & 1;
+        bool w = tm_wait(&full[s], (q / kTmStages) & 1, abort, a.err);
+        w = w && tm_wait(&wempty[b], ((q >> 1) & 1) ^ 1, abort, a.err);
+        if (!__all_sync(kFull, w)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const unsigned char* st = base + s * g.stage;
+        const bool fullres = cc * 16 < a.c1;
+        const uint32_t win = lane_addr + win0 + b * g.win_cols;
+#pragma unroll 1
+        for (int sr = part; sr < g.S; sr += 2) {
+          const int hr = sr + tr;
+          uint32_t c[8], e[8], w0[8], w2[8];
+          tm_slab(st, g, fullres, it.y0, it.x0, hr, tc + 1, c);
+          // the warp's edge lanes fetch the neighbour outside the warp
+          tm_slab(st, g, fullres, it.y0, it.x0, hr, lane == 0 ? tc : tc + 2, e);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            w0[k] = __shfl_up_sync(kFull, c[k], 1);
+            w2[k] = __shfl_down_sync(kFull, c[k], 1);
+            if (lane == 0) w0[k] = e[k];
+            if (lane == 31) w2[k] = e[k];
+          }
+          const uint32_t col = win + (uint32_t)(sr * 3 * 8);
+          tc_st8(col, w0);
+          tc_st8(col + 8, c);
+          tc_st8(col + 16, w2);
+        }
+        tc_wait_st();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) {
+          tm_arrive(&wfull[b]);
+          tm_arrive(&empty[s]);
+        }
+      }
+      if (!ok) break;
+    }
+  } else {
+    // ---- epilogue: thread m reads TMEM lane m
+    const int m = threadIdx.x;
+    const int tr = m / g.tx, tc = m - tr * g.tx;
+    const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
+    uint32_t j = 0;
+    for (int item = blockIdx.x; item < g.items; item += gridDim.x, ++j) {
+      const TmItem it = tm_item(g, item, BN);
+      const uint32_t ab = j % (uint32_t)g.na;
+      if (!__all_sync(kFull, tm_wait(&afull[ab], (j / g.na) & 1, abort, a.err))) break;
+      tc_fence_after();
+      const uint32_t acc = lane_addr + acc0 + ab * g.acc_cols;
+      for (int i = 0; i < g.R; ++i) {
+        const int y = it.y0 + i * g.ty + tr, x = it.x0 + tc;
+        const size_t o0 = (((size_t)it.z * a.H + y) * a.W + x) * a.cout + it.co0;
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+          uint32_t r[16];
+          tc_ld16(acc + (uint32_t)(i * BN + c0), r);
+          uint32_t mk[8];
+          if (a.mask) {
+            const uint4 m0 = *reinterpret_cast<const uint4*>(a.mask + o0 + c0);
+            const uint4 m1v = *reinterpret_cast<const uint4*>(a.mask + o0 + c0 + 8);
+            mk[0] = m0.x; mk[1] = m0.y; mk[2] = m0.z; mk[3] = m0.w;
+            mk[4] = m1v.x; mk[5] = m1v.y; mk[6] = m1v.z; mk[7] = m1v.w;
+          }
+          uint32_t pk[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int co = it.co0 + c0 + 2 * k;
+            float v0 = __uint_as_float(r[2 * k]), v1 = __uint_as_float(r[2 * k + 1]);
+            if (a.bias) {
+              v0 += a.bias[co];
+              v1 += a.bias[co + 1];
+            }
+            if (a.relu) {
+              v0 = fmaxf(v0, 0.f);
+              v1 = fmaxf(v1, 0.f);
+            }
+            if (a.mask) {
+              __nv_bfloat162 mb;
+              memcpy(&mb, &mk[k], 4);
+              if (!(__bfloat162float(mb.x) > 0.f)) v0 = 0.f;
+              if (!(__bfloat162float(mb.y) > 0.f)) v1 = 0.f;
+            }
+            const __nv_bfloat162 o = __floats2bfloat162_rn(v0, v1);
+            memcpy(&pk[k], &o, 4);
+          }
+          *reinterpret_cast<uint4*>(a.y + o0 + c0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          *reinterpret_cast<uint4*>(a.y + o0 + c0 + 8) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tm_arrive(&aempty[ab]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kTmLoadWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmCols));
+}
+#endif
 
 // dW[co][tap][ci] += sum over this block's voxels of dy[v][co] in(v + tap)[ci]
 // (FP32 atomics; the caller zeroes dW).  GEMM M = cout (BM rows per block),
@@ -641,10 +1034,147 @@ static int nn_err(cudaError_t e) {
   clarity::set_last_error(cudaGetErrorString(e));
   return e == cudaErrorMemoryAllocation ? CLARITY_DEVICE_OUT_OF_MEMORY : CLARITY_INVALID_OPERATION;
 }
+// The tcgen05 convolution for widths that are multiples of 32: on unless
+// CLARITY_NN_TCGEN05=0, which selects the mma.sync kernel everywhere;
+// CLARITY_NN_TCGEN05=require makes a call that cannot take it an error.
+enum NnTcMode { kNnTcOff = 0, kNnTcOn = 1, kNnTcRequire = 2 };
+static NnTcMode nn_tcgen05_mode() {
+  static const NnTcMode mode = [] {
+    const char* v = std::getenv("CLARITY_NN_TCGEN05");
+    if (v && v[0] == '0') return kNnTcOff;
+    if (v && std::strcmp(v, "require") == 0) return kNnTcRequire;
+    return kNnTcOn;
+  }();
+  return mode;
+}
 static int nn_bad(const char* m) {
   clarity::set_last_error(m);
   return CLARITY_INVALID_ARGUMENT;
 }
+
+#ifndef CLARITY_HOST_EMULATION
+// Geometry of the tcgen05 convolution for one call, or false when the shape
+// does not suit it (width not a multiple of 32, rows not divisible).
+static bool tm_geometry(const nnk::Conv3Args& a, int* bn_out, nnk::TmGeom* g, int* smem) {
+  const int W = a.W, H = a.H, cout = a.cout;
+  if (W % 32) return false;
+  const int tx = W % 128 == 0 ? 128 : (W % 64 == 0 ? 64 : 32), ty = 128 / tx;
+  const int bn = cout % 128 == 0 ? 128
+                 : cout % 64 == 0 ? 64
+                 : cout % 48 == 0 ? 48
+                 : cout % 32 == 0 ? 32
+                                  : 16;
+  // the most MMA tiles per item (at most 4 rows; one issuing thread each)
+  // whose accumulators and two window buffers fit the 512 TMEM columns, then
+  // two accumulator buffers if they fit
+  int R = 0, na = 0;
+  for (int r = 4; r >= 1 && !R; r /= 2)
+    for (int n = 2; n >= 1 && !R; --n) {
+      if (r * ty > 4 || H % (r * ty)) continue;
+      const int S = (r - 1) * ty + 3;
+      if (n * r * bn + 2 * 24 * S <= nnk::kTmCols) {
+        R = r;
+        na = n;
+      }
+    }
+  if (!R) return false;
+  const int rows = R * ty;
+  nnk::TmGeom& G = *g;
+  G.tx = tx;
+  G.ty = ty;
+  G.R = R;
+  G.rows = rows;
+  G.S = (R - 1) * ty + 3;
+  G.nxb = W / tx;
+  G.nyb = H / rows;
+  G.nnb = cout / bn;
+  const long long items = (long long)G.nxb * G.nyb * a.D * G.nnb;
+  if (items > 0x7fffffffll) return false;
+  G.items = (int)items;
+  G.na = na;
+  G.cw1 = tx + 2;
+  G.cw2 = tx / 2 + 2;
+  const uint32_t halo1 = (uint32_t)((tx + 2) * (rows + 2) * 32);
+  const uint32_t halo2 = (uint32_t)((tx / 2 + 2) * (rows / 2 + 2) * 32);
+  const uint32_t wb = (uint32_t)(2 * 9 * bn * 16);
+  G.wofs = (halo1 + 1023) / 1024 * 1024;
+  G.stage = G.wofs + (wb + 1023) / 1024 * 1024;
+  G.tx1 = halo1 + wb;
+  G.tx2 = halo2 + wb;
+  G.acc_cols = (uint32_t)(R * bn);
+  G.win_cols = (uint32_t)(24 * G.S);
+  // stages, barriers, alignment slack; at least 120 KB so one block holds an SM
+  // (and its 512 TMEM columns) at a time
+  int bytes = nnk::kTmStages * (int)G.stage + 512 + 1024;
+  if (bytes < 120 * 1024) bytes = 120 * 1024;
+  if (bytes > 227 * 1024) return false;
+  *smem = bytes;
+  *bn_out = bn;
+  return true;
+}
+
+static int tm_sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    return 148;
+  return n;
+}
+
+// Launches the tcgen05 convolution.  Returns -1 when the call does not suit
+// it (the caller then takes the mma.sync kernel), else a ClarityResult_t.
+static int tm_conv3(const nnk::Conv3Args& a, cudaStream_t st) {
+  int bn = 0, smem = 0;
+  nnk::TmGeom g{};
+  if (!tm_geometry(a, &bn, &g, &smem)) return -1;
+  using ull = unsigned long long;
+  const int cin = a.c1 + a.c2;
+  clarity::TensorMap m1, m2, mw;
+  {
+    const ull dim[4] = {(ull)a.c1, (ull)a.W, (ull)a.H, (ull)a.D};
+    const ull str[3] = {(ull)a.c1 * 2, (ull)a.W * a.c1 * 2, (ull)a.H * a.W * a.c1 * 2};
+    const unsigned box[4] = {16u, (unsigned)(g.tx + 2), (unsigned)(g.rows + 2), 1u};
+    if (!clarity::encode_tensor_bf16_4d(&m1, a.x1, dim, str, box, true)) return -1;
+  }
+  if (a.c2) {
+    const ull dim[4] = {(ull)a.c2, (ull)a.W2, (ull)a.H2, (ull)a.D2};
+    const ull str[3] = {(ull)a.c2 * 2, (ull)a.W2 * a.c2 * 2, (ull)a.H2 * a.W2 * a.c2 * 2};
+    const unsigned box[4] = {16u, (unsigned)(g.tx / 2 + 2), (unsigned)(g.rows / 2 + 2), 1u};
+    if (!clarity::encode_tensor_bf16_4d(&m2, a.x2, dim, str, box, true)) return -1;
+  } else {
+    m2 = m1;
+  }
+  {
+    // weights [co][27][ci] seen as (ci, co, tap): one box is 8 channels of
+    // BN outputs for 9 taps, landing as 9 tap blocks of BN 16-byte rows
+    const ull dim[4] = {(ull)cin, (ull)a.cout, 27ull, 1ull};
+    const ull str[3] = {27ull * cin * 2, (ull)cin * 2, 27ull * cin * a.cout * 2};
+    const unsigned box[4] = {8u, (unsigned)bn, 9u, 1u};
+    if (!clarity::encode_tensor_bf16_4d(&mw, a.w, dim, str, box, false)) return -1;
+  }
+  const int sms = tm_sm_count();
+  const dim3 grid((unsigned)(g.items < sms ? g.items : sms));
+  cudaError_t e = cudaSuccess;
+  clarity::note_launch_begin(clarity::KK_OTHER, st);
+  switch (bn) {
+#define NN_TM_CASE(B)                                                                        \
+  case B:                                                                                    \
+    e = clarity::smem_opt_in(reinterpret_cast<const void*>(nnk::k_conv3_tm<B>), smem);      \
+    if (e == cudaSuccess)                                                                    \
+      CLARITY_LAUNCH(nnk::k_conv3_tm<B>, grid, nnk::kTmThreads, smem, st)(a, g, m1, m2, mw); \
+    break;
+    NN_TM_CASE(128)
+    NN_TM_CASE(64)
+    NN_TM_CASE(48)
+    NN_TM_CASE(32)
+    NN_TM_CASE(16)
+#undef NN_TM_CASE
+  }
+  clarity::note_launch_end(clarity::KK_OTHER, st);
+  if (e != cudaSuccess) return nn_err(e);
+  return nn_err(cudaGetLastError());
+}
+#endif
 
 extern "C" {
 
@@ -665,6 +1195,15 @@ CLARITY_API ClarityResult_t clarityx_nn_conv3(const void* x1, int c1, const void
                           ((H + nnk::kTY - 1) / nnk::kTY) * ((W + nnk::kTX - 1) / nnk::kTX);
   if (tiles > 0x7fffffffll) return (ClarityResult_t)nn_bad("conv3: volume too large");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (clarity::Context* ctx = clarity::global_context()) a.err = ctx->err_dev();
+#ifndef CLARITY_HOST_EMULATION
+  if (nn_tcgen05_mode() != kNnTcOff) {
+    const int r = tm_conv3(a, st);
+    if (r >= 0) return (ClarityResult_t)r;
+    if (nn_tcgen05_mode() == kNnTcRequire)
+      return (ClarityResult_t)nn_bad("conv3: the tcgen05 kernel cannot take this call (CLARITY_NN_TCGEN05=require)");
+  }
+#endif
   // output channels per block: 48 KB-class shared memory (halo + 27 taps)
   const int bn = cout % 48 == 0 ? 48 : (cout % 32 == 0 ? 32 : 16);
   const dim3 grid((unsigned)tiles, cout / bn);

@@ -192,6 +192,13 @@ __device__ __forceinline__ void prefetch_l2_range(const void* begin, size_t byte
 // the driver rejects it (alignment, extents), so callers can fall back.
 bool encode_tensor_f32_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
                           const unsigned long long stride_bytes[3], const unsigned box[4]);
+// The same for BF16 elements; swizzle32 selects the 32-byte swizzle (16-byte
+// halves of each 32-byte row exchanged when address bit 7 is set), which
+// needs a box whose inner extent is 32 bytes and a 256-byte-aligned
+// destination.  Device builds only.
+bool encode_tensor_bf16_4d(TensorMap* tm, const void* base, const unsigned long long dim[4],
+                           const unsigned long long stride_bytes[3], const unsigned box[4],
+                           bool swizzle32);
 
 // Records `code` in the context's error word.  The word lives in mapped
 // pinned host memory (the host reads it without synchronising the device),

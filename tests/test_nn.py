@@ -31,7 +31,15 @@ def _rand(shape, g, scale=1.0):
 
 @pytest.mark.parametrize("c1,c2,cout,dims", [(16, 0, 16, (8, 12, 16)), (32, 0, 48, (6, 10, 8)),
                                              (16, 32, 64, (8, 8, 12)), (64, 128, 64, (4, 6, 8)),
-                                             (128, 0, 128, (4, 4, 4))])
+                                             (128, 0, 128, (4, 4, 4)),
+                                             # widths that are multiples of 32 take the
+                                             # tcgen05 kernel: 128-, 64- and 32-wide MMA
+                                             # tiles, 1, 2 or 4 rows per item, one or more
+                                             # channel blocks, half-resolution chunks
+                                             (16, 0, 16, (2, 4, 128)), (16, 32, 64, (2, 4, 128)),
+                                             (32, 0, 48, (4, 2, 128)), (64, 0, 128, (2, 2, 256)),
+                                             (16, 0, 80, (2, 4, 128)), (16, 32, 32, (4, 8, 64)),
+                                             (32, 0, 48, (2, 6, 64)), (64, 64, 128, (2, 4, 32))])
 def test_conv3_forward_backward_vs_reference(clarity_gpu, c1, c2, cout, dims):
     from clarity_b200 import unet
     g = torch.Generator().manual_seed(c1 * 7 + c2 + cout)
@@ -80,11 +88,65 @@ def test_conv3_forward_backward_vs_reference(clarity_gpu, c1, c2, cout, dims):
     _close(db, dy.to(torch.float64).sum(dim=(0, 1, 2)), rel=1e-2)
 
 
-def test_conv3_relu_mask_epilogue(clarity_gpu):
+_CROSS = """
+import sys, numpy as np, torch
+from clarity_b200 import unet
+x, w, m = (np.load(sys.argv[i]) for i in (1, 2, 3))
+xd = torch.from_numpy(x).view(torch.bfloat16).cuda()
+wd = torch.from_numpy(w).view(torch.bfloat16).cuda()
+md = torch.from_numpy(m).view(torch.bfloat16).cuda()
+cout = int(sys.argv[5])
+b = torch.linspace(-0.5, 0.5, cout, device="cuda")
+y = unet.conv3(xd, wd, cout, bias=b, relu=True)
+ym = unet.conv3(xd, wd, cout, relu=False, mask=md)
+torch.cuda.synchronize()
+np.save(sys.argv[4], torch.stack([y, ym]).view(torch.int16).cpu().numpy())
+"""
+
+
+@pytest.mark.parametrize("dims,cin,cout", [((4, 4, 256), 32, 64), ((2, 8, 64), 48, 16),
+                                           ((2, 8, 32), 64, 128)])
+def test_conv3_tcgen05_matches_mma_sync_kernel(clarity_gpu, tmp_path, dims, cin, cout):
+    # the same layers through both kernels, each in its own process:
+    # CLARITY_NN_TCGEN05=require (a call the tcgen05 kernel cannot take is an
+    # error, so this proves it ran) and CLARITY_NN_TCGEN05=0 (mma.sync)
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    g = torch.Generator().manual_seed(11 + cin + cout)
+    x = _rand((*dims, cin), g)
+    w = _rand((cout * 27 * cin,), g, 1.0 / np.sqrt(27 * cin))
+    m = _rand((*dims, cout), g)
+    for name, t in (("x", x), ("w", w), ("m", m)):
+        np.save(tmp_path / f"{name}.npy", t.view(torch.int16).numpy())
+    outs = {}
+    for mode in ("require", "0"):
+        env = dict(os.environ, CLARITY_NN_TCGEN05=mode, PYTHONPATH=ROOT)
+        p = subprocess.run([sys.executable, "-c", _CROSS, *(str(tmp_path / f"{n}.npy")
+                                                             for n in "xwm"),
+                            str(tmp_path / f"y{mode}.npy"), str(cout)],
+                           cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr
+        outs[mode] = torch.from_numpy(np.load(tmp_path / f"y{mode}.npy")).view(torch.bfloat16)
+    tc, ms = outs["require"], outs["0"]
+    # FP32 sums in another order, then BF16 rounding: equal or one BF16 step apart
+    _close(tc[0], ms[0], rel=1e-2)
+    _close(tc[1], ms[1], rel=1e-2)
+    assert torch.count_nonzero(tc[0]) > 0
+    # and both against the FP64 reference of the layer
+    wq = w.to(torch.float64).reshape(cout, 27, cin)
+    ref = R.conv3(x.to(torch.float64), wq, cout,
+                  bias=torch.linspace(-0.5, 0.5, cout, dtype=torch.float64), relu=False)
+    _close(tc[0], torch.relu(ref))
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8), (2, 4, 128), (2, 4, 32)])  # both kernels
+def test_conv3_relu_mask_epilogue(clarity_gpu, dims):
     from clarity_b200 import unet
     g = torch.Generator().manual_seed(3)
-    x = _rand((8, 8, 8, 16), g).cuda()
-    m = _rand((8, 8, 8, 16), g).cuda()
+    x = _rand((*dims, 16), g).cuda()
+    m = _rand((*dims, 16), g).cuda()
     w = _rand((16 * 27 * 16,), g, 0.05).cuda()
     y = unet.conv3(x, w, 16, relu=False)
     ym = unet.conv3(x, w, 16, relu=False, mask=m)
