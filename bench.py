@@ -361,7 +361,8 @@ def network_layers(torch, net, shape_zyx=(64, 256, 256), reps=5):
     torch.cuda.synchronize()
     return {"layers": rows, "conv_ms": tot_ms, "conv_tflops": tot_fl / (tot_ms / 1e3) / 1e12,
             "predict_ms": e0.elapsed_time(e1) / reps,
-            "note": "BF16 mma.sync implicit-GEMM convolutions, FP32 accumulation"}
+            "note": "BF16 implicit-GEMM convolutions on tcgen05 (TMEM accumulators, TMA "
+                    "operand loads), FP32 accumulation"}
 
 
 def _cfg2_case(i):

@@ -234,7 +234,9 @@ CLARITY_API ClarityResult_t clarityx_convolve_noalloc(
  * conv3: y = act(bias + 3x3x3 convolution, zero padding) of x1 [D,H,W,c1]
  *   concatenated with x2 [D/2,H/2,W/2,c2] read through nearest upsampling (x2
  *   may be NULL, c2 = 0); act = ReLU when relu, then y *= (mask > 0) when mask
- *   is given.  Tensor cores (mma.sync bf16, FP32 accumulate).
+ *   is given.  Tensor cores, BF16 operands, FP32 accumulation: tcgen05 with
+ *   tensor-memory accumulators when W is a multiple of 32 (unless the
+ *   environment sets CLARITY_NN_TCGEN05=0), else mma.sync.
  * conv3_wgrad: dw[cout][27][cin] += sum_v dy[v][co] in(v + tap)[ci], dbias[co]
  *   += sum_v dy[v][co] (FP32, accumulated: zero them first).
  * conv_in / conv_in_wgrad: the 1 -> 16 first layer (float input, FP32
