@@ -435,39 +435,52 @@ def other_configs(api, torch, stream, n_batch=64, batch_iters=30, cfg3_iters=10)
     psfs = [torch.from_numpy(b).cuda() for _, b in cases]
     outs = [torch.empty_like(a) for a in imgs]
     vox = sum(a.numel() for a in imgs)
-    api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)  # set-up+capture
-    torch.cuda.synchronize()
+    # the schedule's bytes per RL iteration over the batch (2R + Ri + 10C per
+    # volume, as the headline's schedule_bytes), for a bandwidth figure
+    sched = 0
+    for a in imgs:
+        z, y, x = (2 * d for d in a.shape)
+        sched += 2 * 4 * x * y * z + 4 * a.numel() + 10 * 8 * z * y * (x // 2 + 1)
+    peak = peaks()[0]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(3):
-        api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / 3
-    res["batched_rl"] = {"workload": f"{n_batch} volumes of uneven sizes (x, y in 16*{{6..20}}, "
-                                     f"z in 8*{{2..12}}), {batch_iters} RL iterations, one "
-                                     "captured CUDA graph", "image_voxels": int(vox),
-                         "ms": ms, "value": vox * batch_iters / (ms / 1e3) / 1e9,
-                         "unit": "Gvoxel-iter/s", "plans": "planner default"}
-    # the same batch with the autotuner choosing each work box's tiling (the
-    # tuning runs on first use, in the set-up call outside the timed region)
+    desc = (f"{n_batch} volumes of uneven sizes (x, y in 16*{{6..20}}, z in 8*{{2..12}}), "
+            f"{batch_iters} RL iterations")
+
+    def timed(persistent, tuned):
+        if tuned:
+            api.trim()
+            api.autotune(True)
+        try:
+            # set-up (and tuning) and capture, outside the timed region
+            api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream,
+                                persistent=persistent)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(3):
+                api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream,
+                                    persistent=persistent)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        finally:
+            if tuned:
+                api.autotune(False)
+        ms = e0.elapsed_time(e1) / 3
+        gbps = sched * batch_iters / (ms / 1e3) / 1e9
+        return {"workload": desc + (", iterations of all volumes in one persistent launch "
+                                    "(work queue), in one captured CUDA graph" if persistent
+                                    else ", per-volume launches on 8 streams, one captured "
+                                         "CUDA graph"),
+                "image_voxels": int(vox), "ms": ms,
+                "value": vox * batch_iters / (ms / 1e3) / 1e9, "unit": "Gvoxel-iter/s",
+                "schedule_GBps": gbps, "schedule_frac": gbps / peak,
+                "plans": ("autotuned (fastest of the planner's best four tilings per work box)"
+                          if tuned else "planner default")}
+
+    res["batched_rl"] = timed(False, False)
+    res["batched_rl_autotuned"] = timed(False, True)
     api.trim()
-    api.autotune(True)
-    try:
-        api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(3):
-            api.ml_batch_device(imgs, psfs, outs, batch_iters, graph=True, stream=stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    finally:
-        api.autotune(False)
-    ms = e0.elapsed_time(e1) / 3
-    res["batched_rl_autotuned"] = dict(res["batched_rl"], ms=ms,
-                                       value=vox * batch_iters / (ms / 1e3) / 1e9,
-                                       plans="autotuned (fastest of the planner's best four "
-                                             "tilings per work box)")
+    res["batched_rl_persistent"] = timed(True, False)
+    res["batched_rl_persistent_autotuned"] = timed(True, True)
     del imgs, psfs, outs
     img, psf, _ = syn.cfg3()
     di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()

@@ -70,6 +70,7 @@ EXTENSION_SYMBOLS = [
 ]
 DFT_F32, DFT_F16_SPLIT, DFT_BF16_SPLIT = 0, 1, 2
 BATCH_GRAPH = 1  # CLARITYX_BATCH_GRAPH
+BATCH_PERSISTENT = 2  # CLARITYX_BATCH_PERSISTENT
 
 
 class ClarityError(RuntimeError):
@@ -422,11 +423,14 @@ def jvc_device(image, kernel, out, iterations, stream=None):
     return _dev("clarityx_jvc_device", image, kernel, out, [int(iterations)], stream)
 
 
-def ml_batch_device(images, kernels, outs, iterations, graph=True, stream=None):
+def ml_batch_device(images, kernels, outs, iterations, graph=True, stream=None,
+                    persistent=False):
     """clarityx_ml_batch_device: Richardson-Lucy on lists of device tensors
     (volumes of any sizes, one kernel each), run concurrently; with graph the
     batch is captured into a CUDA graph and replayed on later identical
-    calls.  Asynchronous on `stream`."""
+    calls; with persistent the iterations of all volumes run in one
+    persistent launch over a shared work queue.  Asynchronous on
+    `stream`."""
     n = len(images)
     if len(kernels) != n or len(outs) != n:
         raise ValueError("images, kernels and outs must have the same length")
@@ -440,7 +444,9 @@ def ml_batch_device(images, kernels, outs, iterations, graph=True, stream=None):
     ids = (Dim3 * n)(*[dim3(t) for t in images])
     kds = (Dim3 * n)(*[dim3(t) for t in kernels])
     _check(load().clarityx_ml_batch_device(n, imgs, ids, kers, kds, outp, int(iterations),
-                                           BATCH_GRAPH if graph else 0, _stream_ptr(stream)))
+                                           (BATCH_GRAPH if graph else 0) |
+                                           (BATCH_PERSISTENT if persistent else 0),
+                                           _stream_ptr(stream)))
     return outs
 
 

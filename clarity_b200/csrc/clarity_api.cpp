@@ -736,7 +736,8 @@ ClarityResult_t clarityx_ml_batch_device(int count, const float* const* images,
   if (!s.ok()) return report(s);
   ctx->set_stream(static_cast<cudaStream_t>(stream));
   s = clarity::run_rl_batch(*ctx, count, images, ids.data(), kernels, kds.data(), outs,
-                            iterations, (flags & CLARITYX_BATCH_GRAPH) != 0);
+                            iterations, (flags & CLARITYX_BATCH_GRAPH) != 0,
+                            (flags & CLARITYX_BATCH_PERSISTENT) != 0);
   ctx->clear_stream();
   return report(s);
 }

@@ -123,6 +123,7 @@ int static_family_mask() {
 }
 
 static inline void count_small() { g_launches.fetch_add(1); }
+void count_launch() { count_small(); }
 
 static std::atomic<int> g_dft_precision{0};
 void set_dft_precision(int mode) { g_dft_precision.store(mode); }
@@ -498,6 +499,25 @@ void Context::release_workspaces() {
   cudaFree(aux_);
   aux_ = nullptr;
   aux_cap_ = 0;
+  cudaFree(bq_);
+  bq_ = nullptr;
+  bq_cap_ = 0;
+}
+
+Status Context::batch_scratch(size_t bytes, void** out) {
+  if (bq_cap_ < bytes || !bq_) {
+    // graphs captured with the old buffer would use it after it is freed
+    cudaStreamSynchronize(stream_);
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
+    cudaFree(bq_);
+    bq_ = nullptr;
+    bq_cap_ = 0;
+    CL_CHECK(dev_alloc(&bq_, bytes));
+    bq_cap_ = bytes;
+  }
+  *out = bq_;
+  return Status::Ok();
 }
 
 Status Context::aux_scratch(size_t bytes, void** out) {
@@ -1278,10 +1298,20 @@ Status run_rl_accel(Context& ctx, const float* img, Dims id, const float* ker, D
 // volume's solve is issued on batch stream i % nstreams, forked from and
 // joined back to the caller's stream by events, either directly or captured
 // into one CUDA graph that later calls with the same volumes replay.
+// RL set-up of one volume before its first iteration (as rl_solve and
+// rl_core): OTF, energy E = sum of the image, first forward transform.
+static Status rl_prologue(Context& ctx, const PlanEntry& pe, Workspace& ws, const float* img,
+                          Dims id, const float* ker, Dims kd, Dims wd) {
+  CL_TRY(make_otf(ctx, pe, ker, kd, wd, ws.H, nullptr));
+  CL_TRY(reduce_sum_into(ctx, img, id.n(), ws.partial, ws.dscal + 0));
+  return xy_forward(ctx, pe, ProImage{image_src(img, id), pe.P.xmode}, ws.S);
+}
+
 Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* ids,
                     const float* const* kers, const Dims* kds, float* const* outs, int iters,
-                    bool use_graph) {
+                    bool use_graph, bool persistent) {
   if (n <= 0) return Status::Ok();
+  if (iters <= 0) persistent = false;  // nothing to iterate: the copy of rl_solve
 #ifdef CLARITY_HOST_EMULATION
   use_graph = false;  // the emulation runs kernels as they are issued
 #endif
@@ -1303,6 +1333,8 @@ Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* i
     CL_TRY(ctx.workspace_slot(i, *pes[i], ids[i], kds[i], &wss[i]));
   }
   for (int j = 0; j < ns; ++j) CL_TRY(ctx.batch_stream(j, &bs[j]));
+  void* qbuf = nullptr;
+  if (persistent) CL_TRY(ctx.batch_scratch(batch_queue_bytes(n, iters), &qbuf));
   // the caller's stream; a graph is captured on and launched from the
   // context's own stream (capture is not allowed on the legacy default
   // stream), ordered after and before the caller's work by events
@@ -1311,6 +1343,8 @@ Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* i
   std::vector<unsigned long long> key;
   key.push_back((unsigned long long)n);
   key.push_back((unsigned long long)iters);
+  key.push_back(persistent ? 1ull : 0ull);
+  key.push_back((unsigned long long)(uintptr_t)qbuf);
   for (int i = 0; i < n; ++i) {
     for (const void* p : {(const void*)imgs[i], (const void*)kers[i], (const void*)outs[i],
                           (const void*)wss[i]->S, (const void*)wss[i]->H,
@@ -1359,12 +1393,27 @@ Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* i
       for (int j = 0; j < ns; ++j) CL_CHECK(cudaStreamWaitEvent(bs[j], fork, 0));
       for (int i = 0; i < n; ++i) {
         StreamScope scope(ctx, bs[i % ns]);
-        CL_TRY(rl_solve(ctx, *pes[i], *wss[i], imgs[i], ids[i], kers[i], kds[i], wds[i],
-                        outs[i], iters));
+        if (persistent)
+          CL_TRY(rl_prologue(ctx, *pes[i], *wss[i], imgs[i], ids[i], kers[i], kds[i], wds[i]));
+        else
+          CL_TRY(rl_solve(ctx, *pes[i], *wss[i], imgs[i], ids[i], kers[i], kds[i], wds[i],
+                          outs[i], iters));
       }
       for (int j = 0; j < ns; ++j) {
         CL_CHECK(cudaEventRecord(join[j], bs[j]));
         CL_CHECK(cudaStreamWaitEvent(origin, join[j], 0));
+      }
+      if (persistent) {
+        // every volume's iterations in one launch, then the clipped results
+        CL_TRY(launch_rl_batch(ctx, n, pes.data(), wss.data(), imgs, ids, wds.data(), iters,
+                               qbuf, origin));
+        for (int i = 0; i < n; ++i) {
+          count_small();
+          CLARITY_LAUNCH(k_clip, kReduceBlocks, 256, 0, origin)(
+              wss[i]->u, wds[i].x, wds[i].y, outs[i], ids[i].x, ids[i].y, ids[i].z,
+              wss[i]->fscal);
+          CL_CHECK(cudaGetLastError());
+        }
       }
       return Status::Ok();
     };

@@ -108,6 +108,9 @@ class Context {
   // One growable device block for auxiliary scratch (the learned-start
   // network's weights and activations); freed by release_workspaces.
   Status aux_scratch(size_t bytes, void** out);
+  // Queue and tables of the persistent batched launch.  Captured graphs use
+  // it, so growing it first drops every cached graph.
+  Status batch_scratch(size_t bytes, void** out);
   // Reads and clears the error word (no synchronisation: it reports what
   // kernels that have finished recorded).
   Status check_device_errors();
@@ -121,6 +124,8 @@ class Context {
   int* err_dev_ = nullptr;
   void* aux_ = nullptr;
   size_t aux_cap_ = 0;
+  void* bq_ = nullptr;
+  size_t bq_cap_ = 0;
   cudaStream_t user_stream_ = nullptr;
   bool has_user_stream_ = false;
   Status build_entry(const VolPlan& P, std::unique_ptr<PlanEntry>* out);
@@ -179,9 +184,18 @@ Status cast_f32_to_u16(Context& ctx, const float* a, uint16_t* b, long long n);
 // each volume has its own plan and workspace, volumes run concurrently on the
 // batch stream pool, and with use_graph the whole batch is captured into one
 // CUDA graph (replayed when the same batch is run again).
+// persistent: the iterations of all volumes run in one persistent launch
+// (kern_batch.cu) instead of per-volume launches on a pool of streams.
 Status run_rl_batch(Context& ctx, int n, const float* const* imgs, const Dims* ids,
                     const float* const* kers, const Dims* kds, float* const* outs, int iters,
-                    bool use_graph);
+                    bool use_graph, bool persistent = false);
+// The persistent launch (kern_batch.cu): scratch holds batch_queue_bytes(n,
+// iters) bytes; the volumes' set-up (OTF, energy, first forward transform)
+// is already enqueued on st.
+size_t batch_queue_bytes(int n, int iters);
+Status launch_rl_batch(Context& ctx, int n, const PlanEntry* const* pes, Workspace* const* wss,
+                       const float* const* imgs, const Dims* ids, const Dims* wds, int iters,
+                       void* scratch, cudaStream_t st);
 Status run_blind(Context& ctx, const float* img, Dims id, const float* ker,
                  Dims kd, float* out, int iters);
 Status run_jvc(Context& ctx, const float* img, Dims id, const float* ker,
@@ -222,6 +236,8 @@ bool pdl_enabled();
 // a solve launches each kernel hundreds of times).
 cudaError_t smem_opt_in(const void* kernel, int smem);
 long long launch_count();
+// Counts one kernel launch that note_launch_begin/end do not bracket.
+void count_launch();
 int static_family_mask();
 // DFT precision mode of the specialised z pass (0 FP32 register passes, 1
 // split hi+lo FP16 tensor-core first z stage, 2 the same in BF16); applies

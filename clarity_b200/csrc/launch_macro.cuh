@@ -64,3 +64,23 @@ inline PdlLauncher<P...> pdl_launcher(void (*k)(P...), dim3 grid, dim3 block, si
 #define CLARITY_BLOCK_STRIDE(n) ((int)blockDim.x)
 #define CLARITY_ISSUE_LANES ((int)blockDim.x)
 #endif
+
+// The block index and grid size the pass bodies and the operations fused into
+// them see, and the qualifier and load they use for their inputs.  A
+// translation unit may define these before it includes the passes: the
+// persistent batched kernel (kern_batch.cu) runs many work items in one
+// block, so an item's tile stands in for the block and the item's pass for
+// the grid, and it reads data written earlier in the same launch, which
+// needs ordinary coherent loads (no read-only cache, no __restrict__).
+#ifndef CLARITY_BLOCK_ID
+#define CLARITY_BLOCK_ID() blockIdx.x
+#endif
+#ifndef CLARITY_GRID_DIM
+#define CLARITY_GRID_DIM() gridDim.x
+#endif
+#ifndef CLARITY_RESTRICT
+#define CLARITY_RESTRICT __restrict__
+#endif
+#ifndef CLARITY_LDG
+#define CLARITY_LDG(p) __ldg(p)
+#endif

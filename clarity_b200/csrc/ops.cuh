@@ -45,10 +45,10 @@ struct WorkVol {
 // (src/MaximumLikelihoodDeconvolve.cxx:278-282): the image itself inside
 // [0,X)x[0,Y)x[0,Z), zero in the padding.  Only bounds checks, no modulo.
 struct ImageSrc {
-  const float* __restrict__ src;
+  const float* CLARITY_RESTRICT src;
   int X, Y, Z;
   __device__ __forceinline__ float at(int x, int y, int z) const {
-    if (x < X && y < Y && z < Z) return __ldg(&src[((unsigned)z * Y + y) * X + x]);
+    if (x < X && y < Y && z < Z) return CLARITY_LDG(&src[((unsigned)z * Y + y) * X + x]);
     return 0.f;
   }
 };
@@ -58,7 +58,7 @@ struct ImageSrc {
 // work coordinate d maps to s = ((d - shift) wrapped) % dim, inside when
 // s < src dim, otherwise the fill value (0).
 struct PaddedSrc {
-  const float* __restrict__ src;
+  const float* CLARITY_RESTRICT src;
   int X, Y, Z;       // source dims
   int sx, sy, sz;    // shift
   int nx, ny, nz;    // work dims
@@ -72,7 +72,7 @@ struct PaddedSrc {
     const int j = wrap(y, sy, ny);
     const int i = wrap(x, sx, nx);
     if (i >= 0 && j >= 0 && k >= 0 && i < X && j < Y && k < Z)
-      return __ldg(&src[((long long)k * Y + j) * X + i]);
+      return CLARITY_LDG(&src[((long long)k * Y + j) * X + i]);
     return 0.f;
   }
 };
@@ -81,17 +81,17 @@ struct PaddedSrc {
 // Plain work-box volume, optionally multiplied by a device-resident scale
 // (the deferred RL flux rescale).
 struct ProWork {
-  const float* __restrict__ v;
-  const float* __restrict__ scale;  // nullptr -> 1
+  const float* CLARITY_RESTRICT v;
+  const float* CLARITY_RESTRICT scale;  // nullptr -> 1
   WorkVol w;
   int xmode;
   __device__ __forceinline__ float2 load_c(int m, int y, int z) const {
     const float s = scale ? *scale : 1.f;
     if (xmode == 0) {
-      const float2 a = __ldg(reinterpret_cast<const float2*>(v + w.idx(2 * m, y, z)));
+      const float2 a = CLARITY_LDG(reinterpret_cast<const float2*>(v + w.idx(2 * m, y, z)));
       return scale ? make_float2(s * a.x, s * a.y) : a;
     }
-    const float a = __ldg(&v[w.idx(m, y, z)]);
+    const float a = CLARITY_LDG(&v[w.idx(m, y, z)]);
     return make_float2(scale ? s * a : a, 0.f);
   }
   __device__ __forceinline__ void finish() const {}
@@ -101,27 +101,27 @@ struct ProWork {
 // x + alpha (x - xp)), one fused multiply-add, stored to yout on the way into
 // the forward transform (the product step reads it back as the estimate).
 struct ProAccel {
-  const float* __restrict__ x;
-  const float* __restrict__ xp;
-  const float* __restrict__ alpha;
-  float* __restrict__ yout;
+  const float* CLARITY_RESTRICT x;
+  const float* CLARITY_RESTRICT xp;
+  const float* CLARITY_RESTRICT alpha;
+  float* CLARITY_RESTRICT yout;
   WorkVol w;
   int xmode;
   __device__ __forceinline__ static float extrap(float a, float x, float xp) {
     return fmaxf(0.f, fmaf(a, x - xp, x));
   }
   __device__ __forceinline__ float2 load_c(int m, int y, int z) const {
-    const float a = __ldg(alpha);
+    const float a = CLARITY_LDG(alpha);
     if (xmode == 0) {
       const unsigned i = w.idx(2 * m, y, z);
-      const float2 xv = __ldg(reinterpret_cast<const float2*>(x + i));
-      const float2 pv = __ldg(reinterpret_cast<const float2*>(xp + i));
+      const float2 xv = CLARITY_LDG(reinterpret_cast<const float2*>(x + i));
+      const float2 pv = CLARITY_LDG(reinterpret_cast<const float2*>(xp + i));
       const float2 r = make_float2(extrap(a, xv.x, pv.x), extrap(a, xv.y, pv.y));
       *reinterpret_cast<float2*>(yout + i) = r;
       return r;
     }
     const unsigned i = w.idx(m, y, z);
-    const float r = extrap(a, __ldg(x + i), __ldg(xp + i));
+    const float r = extrap(a, CLARITY_LDG(x + i), CLARITY_LDG(xp + i));
     yout[i] = r;
     return make_float2(r, 0.f);
   }
@@ -131,7 +131,7 @@ struct ProAccel {
 // Unpadded source read through the pad/shift map, times an optional scale.
 struct ProPadded {
   PaddedSrc p;
-  const float* __restrict__ scale;  // nullptr -> 1
+  const float* CLARITY_RESTRICT scale;  // nullptr -> 1
   int xmode;
   __device__ __forceinline__ float2 load_c(int m, int y, int z) const {
     const float s = scale ? *scale : 1.f;
@@ -159,7 +159,7 @@ struct ProImage {
 };
 
 // ---------------------------------------------------------------- epilogues
-// Block-wide FP64 sum of per-thread partials into partial[blockIdx.x]
+// Block-wide FP64 sum of per-thread partials into partial[block index]
 // (fixed reduction order: deterministic).
 __device__ __forceinline__ void block_sum_store(double acc, double* partial) {
   __shared__ double red[32];
@@ -174,7 +174,7 @@ __device__ __forceinline__ void block_sum_store(double acc, double* partial) {
     double a = lane < nw ? red[lane] : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0) partial[blockIdx.x] = a;
+    if (lane == 0) partial[CLARITY_BLOCK_ID()] = a;
   }
 }
 
@@ -201,7 +201,7 @@ __device__ __forceinline__ double block_total(const double* partial, int np) {
 // Store the real-space result on the work box.
 struct EpiWork {
   static constexpr bool has_zero_rows = false;
-  float* __restrict__ out;
+  float* CLARITY_RESTRICT out;
   WorkVol w;
   int xmode;
   __device__ __forceinline__ float2 apply_c(int m, int y, int z, float2 c) {
@@ -224,9 +224,9 @@ struct EpiWork {
 // into an unpadded (X, Y, Z) volume, times an optional device scale.
 struct EpiClip {
   static constexpr bool has_zero_rows = false;
-  float* __restrict__ out;
+  float* CLARITY_RESTRICT out;
   int X, Y, Z;
-  const float* __restrict__ scale;
+  const float* CLARITY_RESTRICT scale;
   int xmode;
   __device__ __forceinline__ void put(int x, int y, int z, float v) {
     if (x < X && y < Y && z < Z) {
@@ -258,18 +258,18 @@ struct EpiClip {
 struct EpiRLProduct {
   static constexpr bool has_zero_rows = false;
   static constexpr int kFamily = KK_XY_PRODUCT;
-  const float* __restrict__ cur;     // work-box estimate, or nullptr
+  const float* CLARITY_RESTRICT cur;     // work-box estimate, or nullptr
   ImageSrc g;                        // used when cur == nullptr
-  const float* __restrict__ scale;   // deferred flux scale for cur
-  float* __restrict__ unew;
-  double* __restrict__ partial;
+  const float* CLARITY_RESTRICT scale;   // deferred flux scale for cur
+  float* CLARITY_RESTRICT unew;
+  double* CLARITY_RESTRICT partial;
   WorkVol w;
   int xmode;
   double acc;
   int* nblocks = nullptr;  // receives the grid size (the number of partials), or nullptr
   __device__ __forceinline__ float cur_at(int x, int y, int z) const {
     if (cur) {
-      const float u = __ldg(&cur[w.idx(x, y, z)]);
+      const float u = CLARITY_LDG(&cur[w.idx(x, y, z)]);
       return scale ? *scale * u : u;
     }
     return g.at(x, y, z);
@@ -312,7 +312,7 @@ struct EpiRLProduct {
     const int x = 2 * m;
     float u0 = x < n ? sr[x] : 0.f, u1 = x + 1 < n ? sr[x + 1] : 0.f;
     if (cur && scale) {
-      const float s = __ldg(scale);
+      const float s = CLARITY_LDG(scale);
       u0 = s * u0;
       u1 = s * u1;
     }
@@ -325,7 +325,7 @@ struct EpiRLProduct {
   }
   __device__ __forceinline__ void finish() {
     block_sum_store(acc, partial);
-    if (nblocks && blockIdx.x == 0 && threadIdx.x == 0) *nblocks = (int)gridDim.x;
+    if (nblocks && CLARITY_BLOCK_ID() == 0 && threadIdx.x == 0) *nblocks = (int)CLARITY_GRID_DIM();
   }
 };
 
@@ -340,7 +340,7 @@ struct MidRLRatio {
   // g > 0 >= b skipped), summed in FP64 per block; block 0 stores the grid
   // size in *nblocks.  Same definition as k_idiv and the oracle
   // (IDIVFunctional, src/IDivergenceDeconvolve.cxx:33-47, alpha = 0).
-  double* __restrict__ idiv_partial = nullptr;
+  double* CLARITY_RESTRICT idiv_partial = nullptr;
   int* nblocks = nullptr;
   double acc = 0.0;
   __device__ __forceinline__ void idiv_add(float a, float b) {
@@ -403,14 +403,14 @@ struct MidRLRatio {
   __device__ __forceinline__ void finish() {
     if (idiv_partial) {
       block_sum_store(acc, idiv_partial);
-      if (nblocks && blockIdx.x == 0 && threadIdx.x == 0) *nblocks = (int)gridDim.x;
+      if (nblocks && CLARITY_BLOCK_ID() == 0 && threadIdx.x == 0) *nblocks = (int)CLARITY_GRID_DIM();
     }
   }
   // a block that returned early (plane outside the image) contributes zero
   __device__ __forceinline__ void finish_skipped() {
     if (idiv_partial && threadIdx.x == 0) {
-      idiv_partial[blockIdx.x] = 0.0;
-      if (nblocks && blockIdx.x == 0) *nblocks = (int)gridDim.x;
+      idiv_partial[CLARITY_BLOCK_ID()] = 0.0;
+      if (nblocks && CLARITY_BLOCK_ID() == 0) *nblocks = (int)CLARITY_GRID_DIM();
     }
   }
 };
@@ -422,9 +422,9 @@ struct MidRLRatio {
 // fused kernel transforms it for the next iteration.
 struct EpiJVC {
   static constexpr bool has_zero_rows = false;
-  const float* __restrict__ cur;
+  const float* CLARITY_RESTRICT cur;
   ImageSrc g;
-  float* __restrict__ inext;
+  float* CLARITY_RESTRICT inext;
   float A, invASq;
   WorkVol w;
   int xmode;
@@ -438,14 +438,14 @@ struct EpiJVC {
     if (xmode == 0) {
       const int x = 2 * m;
       const float g0 = g.at(x, y, z), g1 = g.at(x + 1, y, z);
-      const float i0 = cur ? __ldg(&cur[w.idx(x, y, z)]) : g0;
-      const float i1 = cur ? __ldg(&cur[w.idx(x + 1, y, z)]) : g1;
+      const float i0 = cur ? CLARITY_LDG(&cur[w.idx(x, y, z)]) : g0;
+      const float i1 = cur ? CLARITY_LDG(&cur[w.idx(x + 1, y, z)]) : g1;
       const float2 r = make_float2(upd(i0, g0, o.x), upd(i1, g1, o.y));
       *reinterpret_cast<float2*>(inext + w.idx(x, y, z)) = r;
       return r;
     }
     const float g0 = g.at(m, y, z);
-    const float i0 = cur ? __ldg(&cur[w.idx(m, y, z)]) : g0;
+    const float i0 = cur ? CLARITY_LDG(&cur[w.idx(m, y, z)]) : g0;
     const float r = upd(i0, g0, o.x);
     inext[w.idx(m, y, z)] = r;
     return make_float2(r, 0.f);
@@ -472,9 +472,9 @@ struct EpiJVC {
 // transformed before its scale was known.
 struct ModOTF {
   static constexpr bool forward_only = false;
-  const float2* __restrict__ H;
+  const float2* CLARITY_RESTRICT H;
   float scale;
-  const float* __restrict__ scale2 = nullptr;
+  const float* CLARITY_RESTRICT scale2 = nullptr;
   // only the first zn z planes of the input spectrum are nonzero (the rest
   // were never written and are read as zeros)
   int zn = 1 << 30;
@@ -490,7 +490,7 @@ struct ModOTF {
                         off + chunk <= total ? chunk : total - off);
   }
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
-    const float2 h = __ldg(&H[idx]);
+    const float2 h = CLARITY_LDG(&H[idx]);
     const float f = scale2 ? scale * *scale2 : scale;
     return make_float2(f * (v.x * h.x - v.y * h.y), f * (v.x * h.y + v.y * h.x));
   }
@@ -498,7 +498,7 @@ struct ModOTF {
   __device__ __forceinline__ ModOTF resolved() const {
     ModOTF r = *this;
     if (scale2) {
-      r.scale = scale * __ldg(scale2);
+      r.scale = scale * CLARITY_LDG(scale2);
       r.scale2 = nullptr;
     }
     return r;
@@ -509,7 +509,7 @@ struct ModOTF {
 // scale * (that * G).
 struct ModWiener {
   static constexpr bool forward_only = false;
-  const float2* __restrict__ H;
+  const float2* CLARITY_RESTRICT H;
   float eps, scale;
   int zn = 1 << 30;
   int zout = 1 << 30;
@@ -521,7 +521,7 @@ struct ModWiener {
                         off + chunk <= total ? chunk : total - off);
   }
   __device__ __forceinline__ float2 apply(long long idx, float2 v) const {
-    const float2 h = __ldg(&H[idx]);
+    const float2 h = CLARITY_LDG(&H[idx]);
     const float mag = h.x * h.x + h.y * h.y;
     const float f = 1.0f / (mag + eps);
     const float a = h.x * f, b = -h.y * f;

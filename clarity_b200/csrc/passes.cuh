@@ -35,7 +35,7 @@ template <int R, int DIR, bool PADX>
 __device__ __forceinline__ void smem_pass(float2* sm, const VolPlan& P,
                                           const AxisPlan& A, int s, int nlines,
                                           int l0n, int s0, int s1, int es,
-                                          bool l0fast, const float2* __restrict__ tw) {
+                                          bool l0fast, const float2* CLARITY_RESTRICT tw) {
   const int n = A.n;
   const int len = A.len[s];
   const int span = A.span[s];
@@ -68,12 +68,12 @@ __device__ __forceinline__ void smem_pass(float2* sm, const VolPlan& P,
       dft<R, -1>(v);
       if (i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k * twstep]));
+        for (int k = 1; k < R; ++k) v[k] = cmul(v[k], CLARITY_LDG(&tw[i * k * twstep]));
       }
     } else {
       if (i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k * twstep]));
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], CLARITY_LDG(&tw[i * k * twstep]));
       }
       dft<R, +1>(v);
     }
@@ -136,7 +136,7 @@ __device__ __forceinline__ void smem_inverse(float2* sm, const VolPlan& P,
 template <int R, class Pro>
 __device__ __forceinline__ void x_first_pass(float2* sm, const VolPlan& P,
                                              const Pro& pro, int z, int y0base,
-                                             const float2* __restrict__ tw) {
+                                             const float2* CLARITY_RESTRICT tw) {
   const AxisPlan& A = P.ax;
   const int span = A.span[0];
   const int rows = P.G * P.Ay;
@@ -152,7 +152,7 @@ __device__ __forceinline__ void x_first_pass(float2* sm, const VolPlan& P,
     dft<R, -1>(v);
     if (i != 0) {
 #pragma unroll
-      for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k]));
+      for (int k = 1; k < R; ++k) v[k] = cmul(v[k], CLARITY_LDG(&tw[i * k]));
     }
     float2* row = sm + r * P.rowStride;
 #pragma unroll
@@ -192,16 +192,16 @@ __device__ __forceinline__ unsigned k1_stride(const VolPlan& P) {
 
 template <int AY>
 __device__ __forceinline__ void col_split_store(float2* v, const VolPlan& P,
-                                                float2* __restrict__ S, int kx,
+                                                float2* CLARITY_RESTRICT S, int kx,
                                                 int z, int y0,
-                                                const float2* __restrict__ twny) {
+                                                const float2* CLARITY_RESTRICT twny) {
   dft<AY, -1>(v);
   float2* dst = S + s_base(P, kx, z, y0);
   const unsigned ks = k1_stride(P);
 #pragma unroll
   for (int k1 = 0; k1 < AY; ++k1) {
     float2 w = (k1 == 0 || y0 == 0) ? make_float2(1.f, 0.f)
-                                    : __ldg(&twny[y0 * k1]);
+                                    : CLARITY_LDG(&twny[y0 * k1]);
     dst[k1 * ks] = cmul(v[k1], w);
   }
 }
@@ -209,10 +209,10 @@ __device__ __forceinline__ void col_split_store(float2* v, const VolPlan& P,
 template <int AY>
 __device__ __forceinline__ void r2c_cols_forward(const float2* sm,
                                                  const VolPlan& P,
-                                                 float2* __restrict__ S, int z,
+                                                 float2* CLARITY_RESTRICT S, int z,
                                                  int y0base,
-                                                 const float2* __restrict__ tw,
-                                                 const int* __restrict__ xrev) {
+                                                 const float2* CLARITY_RESTRICT tw,
+                                                 const int* CLARITY_RESTRICT xrev) {
   const float2* twr = tw + P.tw_r2c_off;
   const float2* twny = tw + P.tw_ny_off;
   const int total = P.G * P.items;
@@ -222,7 +222,7 @@ __device__ __forceinline__ void r2c_cols_forward(const float2* sm,
     const int y0 = y0base + g;
     const float2* rows = sm + (g * AY) * P.rowStride;
     if (P.xmode == 1) {
-      const int pk = xpos(P, __ldg(&xrev[it]));
+      const int pk = xpos(P, CLARITY_LDG(&xrev[it]));
       float2 a[AY];
 #pragma unroll
       for (int j = 0; j < AY; ++j) a[j] = rows[j * P.rowStride + pk];
@@ -243,7 +243,7 @@ __device__ __forceinline__ void r2c_cols_forward(const float2* sm,
         col_split_store<AY>(xc, P, S, side == 0 ? 0 : M, z, y0, twny);
       }
       if ((M & 1) == 0 && M >= 2) {
-        const int ph = xpos(P, __ldg(&xrev[M / 2]));
+        const int ph = xpos(P, CLARITY_LDG(&xrev[M / 2]));
         float2 xh[AY];
 #pragma unroll
         for (int j = 0; j < AY; ++j) xh[j] = conjf2(rows[j * P.rowStride + ph]);
@@ -253,9 +253,9 @@ __device__ __forceinline__ void r2c_cols_forward(const float2* sm,
       // pair (k, M-k); one output column at a time keeps register use at
       // one column of Ay values
       const int k = it;
-      const int pa = xpos(P, __ldg(&xrev[k]));
-      const int pb = xpos(P, __ldg(&xrev[M - k]));
-      const float2 w = __ldg(&twr[k]);
+      const int pa = xpos(P, CLARITY_LDG(&xrev[k]));
+      const int pb = xpos(P, CLARITY_LDG(&xrev[M - k]));
+      const float2 w = CLARITY_LDG(&twr[k]);
 #pragma unroll 1
       for (int side = 0; side < 2; ++side) {
         float2 xc[AY];
@@ -280,15 +280,15 @@ __device__ __forceinline__ void r2c_cols_forward(const float2* sm,
 // c2r pre-processing, write digit-reversed rows into smem.
 template <int AY>
 __device__ __forceinline__ void col_split_load(float2* v, const VolPlan& P,
-                                               const float2* __restrict__ S,
+                                               const float2* CLARITY_RESTRICT S,
                                                int kx, int z, int y0,
-                                               const float2* __restrict__ twny) {
+                                               const float2* CLARITY_RESTRICT twny) {
   const float2* src = S + s_base(P, kx, z, y0);
   const unsigned ks = k1_stride(P);
 #pragma unroll
   for (int k1 = 0; k1 < AY; ++k1) {
-    float2 a = __ldg(&src[k1 * ks]);
-    if (k1 != 0 && y0 != 0) a = cmulc(a, __ldg(&twny[y0 * k1]));
+    float2 a = CLARITY_LDG(&src[k1 * ks]);
+    if (k1 != 0 && y0 != 0) a = cmulc(a, CLARITY_LDG(&twny[y0 * k1]));
     v[k1] = a;
   }
   dft<AY, +1>(v);
@@ -296,10 +296,10 @@ __device__ __forceinline__ void col_split_load(float2* v, const VolPlan& P,
 
 template <int AY>
 __device__ __forceinline__ void c2r_cols_inverse(float2* sm, const VolPlan& P,
-                                                 const float2* __restrict__ S,
+                                                 const float2* CLARITY_RESTRICT S,
                                                  int z, int y0base,
-                                                 const float2* __restrict__ tw,
-                                                 const int* __restrict__ xrev) {
+                                                 const float2* CLARITY_RESTRICT tw,
+                                                 const int* CLARITY_RESTRICT xrev) {
   const float2* twr = tw + P.tw_r2c_off;
   const float2* twny = tw + P.tw_ny_off;
   const int total = P.G * P.items;
@@ -309,7 +309,7 @@ __device__ __forceinline__ void c2r_cols_inverse(float2* sm, const VolPlan& P,
     const int y0 = y0base + g;
     float2* rows = sm + (g * AY) * P.rowStride;
     if (P.xmode == 1) {
-      const int pk = xpos(P, __ldg(&xrev[it]));
+      const int pk = xpos(P, CLARITY_LDG(&xrev[it]));
       float2 a[AY];
       col_split_load<AY>(a, P, S, it, z, y0, twny);
 #pragma unroll
@@ -338,7 +338,7 @@ __device__ __forceinline__ void c2r_cols_inverse(float2* sm, const VolPlan& P,
       if ((M & 1) == 0 && M >= 2) {
         float2 xh[AY];
         col_split_load<AY>(xh, P, S, M / 2, z, y0, twny);
-        const int ph = xpos(P, __ldg(&xrev[M / 2]));
+        const int ph = xpos(P, CLARITY_LDG(&xrev[M / 2]));
 #pragma unroll
         for (int j = 0; j < AY; ++j)
           rows[j * P.rowStride + ph] = make_float2(2.f * xh[j].x, -2.f * xh[j].y);
@@ -347,8 +347,8 @@ __device__ __forceinline__ void c2r_cols_inverse(float2* sm, const VolPlan& P,
       // pair (k, M-k): inverse-transform each column into its own smem
       // slot, then combine the two slots in place (same thread, no sync)
       const int k = it;
-      const int pa = xpos(P, __ldg(&xrev[k]));
-      const int pb = xpos(P, __ldg(&xrev[M - k]));
+      const int pa = xpos(P, CLARITY_LDG(&xrev[k]));
+      const int pb = xpos(P, CLARITY_LDG(&xrev[M - k]));
       {
         float2 xc[AY];
         col_split_load<AY>(xc, P, S, k, z, y0, twny);
@@ -361,7 +361,7 @@ __device__ __forceinline__ void c2r_cols_inverse(float2* sm, const VolPlan& P,
 #pragma unroll
         for (int j = 0; j < AY; ++j) rows[j * P.rowStride + pb] = xc[j];
       }
-      const float2 w = __ldg(&twr[k]);
+      const float2 w = CLARITY_LDG(&twr[k]);
 #pragma unroll 4
       for (int j = 0; j < AY; ++j) {
         const float2 xa = rows[j * P.rowStride + pa];
@@ -405,7 +405,7 @@ __device__ __noinline__ void cols_rt(float2* sm, const VolPlan& P, float2* S,
 template <int R, class Epi, bool FUSE>
 __device__ __forceinline__ void x_last_pass(float2* sm, const VolPlan& P,
                                             Epi& epi, int z, int y0base,
-                                            const float2* __restrict__ tw) {
+                                            const float2* CLARITY_RESTRICT tw) {
   const AxisPlan& A = P.ax;
   const int span = A.npass > 0 ? A.span[0] : 1;
   const int rows = P.G * P.Ay;
@@ -422,7 +422,7 @@ __device__ __forceinline__ void x_last_pass(float2* sm, const VolPlan& P,
     if (A.npass > 0) {
       if (i != 0) {
 #pragma unroll
-        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], __ldg(&tw[i * k]));
+        for (int k = 1; k < R; ++k) v[k] = cmulc(v[k], CLARITY_LDG(&tw[i * k]));
       }
       dft<R, +1>(v);
     }
@@ -433,7 +433,7 @@ __device__ __forceinline__ void x_last_pass(float2* sm, const VolPlan& P,
         dft<R, -1>(v);
         if (i != 0) {
 #pragma unroll
-          for (int k = 1; k < R; ++k) v[k] = cmul(v[k], __ldg(&tw[i * k]));
+          for (int k = 1; k < R; ++k) v[k] = cmul(v[k], CLARITY_LDG(&tw[i * k]));
         }
       }
 #pragma unroll
@@ -483,16 +483,19 @@ __device__ __forceinline__ void x_first_pass_rt(float2* sm, const VolPlan& P,
 }
 
 // ------------------------------------------------------------------------
-// Kernels.  Grid: XY kernels use blockIdx.x over (z, y0 group):
-// z = blockIdx.x / (By/G), y0base = (blockIdx.x % (By/G)) * G.
+// Pass bodies.  XY bodies take one (z, y0 group) tile, bid over
+// z = bid / (By/G), y0base = (bid % (By/G)) * G; Z bodies take the tile
+// S[k1][kg] at bid = k1*KG + kg.  The kernels below run one body per block
+// (bid = blockIdx.x); the persistent batched kernel (kern_batch.cu) runs
+// many, one per work item.
 template <class Pro>
-__global__ void __launch_bounds__(256, 2)
-    k_xy_forward(const VolPlan P, const Pro pro, float2* __restrict__ S,
-                 const float2* __restrict__ tw, const int* __restrict__ xrev) {
-  CLARITY_DYN_SMEM(float2, sm);
+__device__ __forceinline__ void xy_forward_body(float2* sm, const VolPlan& P, const Pro& pro,
+                                                float2* CLARITY_RESTRICT S,
+                                                const float2* CLARITY_RESTRICT tw,
+                                                const int* CLARITY_RESTRICT xrev, int bid) {
   const int ngroups = P.By / P.G;
-  const int z = blockIdx.x / ngroups;
-  const int y0base = (blockIdx.x - z * ngroups) * P.G;
+  const int z = bid / ngroups;
+  const int y0base = (bid - z * ngroups) * P.G;
   const float2* twx = tw + P.ax.tw_off;
   x_first_pass_rt(sm, P, pro, z, y0base, twx);
   __syncthreads();
@@ -502,13 +505,13 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <class Epi>
-__global__ void __launch_bounds__(256, 2)
-    k_xy_inverse(const VolPlan P, Epi epi, const float2* __restrict__ S,
-                 const float2* __restrict__ tw, const int* __restrict__ xrev) {
-  CLARITY_DYN_SMEM(float2, sm);
+__device__ __forceinline__ void xy_inverse_body(float2* sm, const VolPlan& P, Epi& epi,
+                                                const float2* CLARITY_RESTRICT S,
+                                                const float2* CLARITY_RESTRICT tw,
+                                                const int* CLARITY_RESTRICT xrev, int bid) {
   const int ngroups = P.By / P.G;
-  const int z = blockIdx.x / ngroups;
-  const int y0base = (blockIdx.x - z * ngroups) * P.G;
+  const int z = bid / ngroups;
+  const int y0base = (bid - z * ngroups) * P.G;
   const float2* twx = tw + P.ax.tw_off;
   cols_rt<false>(sm, P, const_cast<float2*>(S), z, y0base, tw, xrev);
   __syncthreads();
@@ -518,19 +521,19 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 // Inverse x/y transform, point-wise operation, forward transform: one pass.
-// Reads and writes S in place (each block owns its (z, y0-group) slice).
+// Reads and writes S in place (each tile owns its (z, y0-group) slice).
 template <class Mid>
-__global__ void __launch_bounds__(256, 2)
-    k_xy_inv_fwd(const VolPlan P, Mid mid, float2* __restrict__ S,
-                 const float2* __restrict__ tw, const int* __restrict__ xrev) {
-  CLARITY_DYN_SMEM(float2, sm);
+__device__ __forceinline__ void xy_inv_fwd_body(float2* sm, const VolPlan& P, Mid& mid,
+                                                float2* CLARITY_RESTRICT S,
+                                                const float2* CLARITY_RESTRICT tw,
+                                                const int* CLARITY_RESTRICT xrev, int bid) {
   const int ngroups = P.By / P.G;
-  const int z = blockIdx.x / ngroups;
-  const int y0base = (blockIdx.x - z * ngroups) * P.G;
+  const int z = bid / ngroups;
+  const int y0base = (bid - z * ngroups) * P.G;
   const float2* twx = tw + P.ax.tw_off;
   // a plane whose result is known to be zero is neither read nor written;
   // the next Z pass reads those planes as zeros (Mod::zn)
-  if (mid.zero_plane(z)) {  // neither read nor written (see Mod::zn)
+  if (mid.zero_plane(z)) {
     if constexpr (requires { mid.finish_skipped(); }) mid.finish_skipped();
     return;
   }
@@ -549,12 +552,12 @@ __global__ void __launch_bounds__(256, 2)
 // OTF and the Wiener numerator); otherwise Mod::apply(idx, v) runs between the
 // forward and inverse transforms, idx being the element's offset in S.
 template <class Mod>
-__global__ void __launch_bounds__(256, 2)
-    k_z(const VolPlan P, const Mod mod, const float2* __restrict__ Sin,
-        float2* __restrict__ Sout, const float2* __restrict__ tw) {
-  CLARITY_DYN_SMEM(float2, sm);
+__device__ __forceinline__ void z_body(float2* sm, const VolPlan& P, const Mod& mod,
+                                       const float2* CLARITY_RESTRICT Sin,
+                                       float2* CLARITY_RESTRICT Sout,
+                                       const float2* CLARITY_RESTRICT tw, int bid) {
   const long long tile = (long long)P.nz * P.By * P.W;
-  const long long base = (long long)blockIdx.x * tile;
+  const long long base = (long long)bid * tile;
   // load (16-byte vectors when the tile size is even, which keeps every
   // tile base 16-byte aligned)
   // planes z >= zn of the input are zero (not read)
@@ -564,7 +567,7 @@ __global__ void __launch_bounds__(256, 2)
     float4* dst = reinterpret_cast<float4*>(sm);
     const int n4 = (int)(tile / 2), live4 = (int)(live / 2);
     for (int t = threadIdx.x; t < n4; t += blockDim.x)
-      dst[t] = t < live4 ? __ldg(&src[t]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      dst[t] = t < live4 ? CLARITY_LDG(&src[t]) : make_float4(0.f, 0.f, 0.f, 0.f);
   } else {
     for (int t = threadIdx.x; t < tile; t += blockDim.x)
       sm[t] = t < live ? Sin[base + t] : make_float2(0.f, 0.f);
@@ -594,6 +597,40 @@ __global__ void __launch_bounds__(256, 2)
   } else {
     for (int t = threadIdx.x; t < out; t += blockDim.x) Sout[base + t] = sm[t];
   }
+}
+
+// ------------------------------------------------------------------------
+// Kernels: one body per block.
+template <class Pro>
+__global__ void __launch_bounds__(256, 2)
+    k_xy_forward(const VolPlan P, const Pro pro, float2* CLARITY_RESTRICT S,
+                 const float2* CLARITY_RESTRICT tw, const int* CLARITY_RESTRICT xrev) {
+  CLARITY_DYN_SMEM(float2, sm);
+  xy_forward_body(sm, P, pro, S, tw, xrev, (int)blockIdx.x);
+}
+
+template <class Epi>
+__global__ void __launch_bounds__(256, 2)
+    k_xy_inverse(const VolPlan P, Epi epi, const float2* CLARITY_RESTRICT S,
+                 const float2* CLARITY_RESTRICT tw, const int* CLARITY_RESTRICT xrev) {
+  CLARITY_DYN_SMEM(float2, sm);
+  xy_inverse_body(sm, P, epi, S, tw, xrev, (int)blockIdx.x);
+}
+
+template <class Mid>
+__global__ void __launch_bounds__(256, 2)
+    k_xy_inv_fwd(const VolPlan P, Mid mid, float2* CLARITY_RESTRICT S,
+                 const float2* CLARITY_RESTRICT tw, const int* CLARITY_RESTRICT xrev) {
+  CLARITY_DYN_SMEM(float2, sm);
+  xy_inv_fwd_body(sm, P, mid, S, tw, xrev, (int)blockIdx.x);
+}
+
+template <class Mod>
+__global__ void __launch_bounds__(256, 2)
+    k_z(const VolPlan P, const Mod mod, const float2* CLARITY_RESTRICT Sin,
+        float2* CLARITY_RESTRICT Sout, const float2* CLARITY_RESTRICT tw) {
+  CLARITY_DYN_SMEM(float2, sm);
+  z_body(sm, P, mod, Sin, Sout, tw, (int)blockIdx.x);
 }
 
 }  // namespace clarity

@@ -145,10 +145,18 @@ CLARITY_API ClarityResult_t clarityx_ml_accel_device(
  * workspace and the volumes run concurrently on a pool of streams, forked
  * from and joined back to `stream`.  flags & CLARITYX_BATCH_GRAPH captures the
  * whole batch into one CUDA graph, kept and replayed when the same batch
- * (same pointers, sizes and iterations) is run again.  Asynchronous like the
- * other _device calls.  Extension of Clarity_MaximumLikelihoodDeconvolve
- * (Clarity.h.in:337-341), which takes one volume. */
+ * (same pointers, sizes and iterations) is run again.
+ * flags & CLARITYX_BATCH_PERSISTENT runs the iterations of all volumes in one
+ * persistent launch: a fixed grid of blocks takes tiles of every volume's
+ * passes from one work queue (each volume's set-up and its clipped result
+ * are ordinary launches around it).  The iterations then use the
+ * runtime-planned pass kernels for every work box, so a box that has
+ * specialised kernels can differ from its single-volume solve in the last
+ * bits.  Asynchronous like the other _device calls.  Extension of
+ * Clarity_MaximumLikelihoodDeconvolve (Clarity.h.in:337-341), which takes
+ * one volume. */
 #define CLARITYX_BATCH_GRAPH 1
+#define CLARITYX_BATCH_PERSISTENT 2
 CLARITY_API ClarityResult_t clarityx_ml_batch_device(
     int count, const float *const *images, const Clarity_Dim3 *imageDims,
     const float *const *kernels, const Clarity_Dim3 *kernelDims,

@@ -95,6 +95,11 @@ inline T __ldcg(const T* p) {
   return *p;
 }
 // one thread per block: atomics are plain read-modify-writes
+inline int atomicAdd(int* p, int v) {
+  const int o = *p;
+  *p = o + v;
+  return o;
+}
 inline unsigned atomicAdd(unsigned* p, unsigned v) {
   const unsigned o = *p;
   *p = o + v;

@@ -112,6 +112,32 @@ def test_emulated_library_matches_oracle(emu, tmp_path, oracle_lib, img_zyx, psf
     # emu_main), the first against the oracle
     assert rel_l2(run_emu(emu, tmp_path, "batch", img, psf, 2),
                   oracle_lib.rl(img, psf, 2)) <= 2e-6
+    # the persistent batched launch: the same three volumes through one work
+    # queue (checked against the single solves in emu_main), the first
+    # against the oracle
+    assert rel_l2(run_emu(emu, tmp_path, "batchp", img, psf, 3),
+                  oracle_lib.rl(img, psf, 3)) <= 2e-6
+
+
+@pytest.mark.parametrize("img_zyx,psf_zyx", [((16, 32, 32), (16, 32, 32)),
+                                             ((12, 24, 20), (12, 24, 20)),
+                                             ((6, 9, 10), (3, 4, 5))])
+def test_emulated_persistent_batch_equals_single_solves(emu, tmp_path, img_zyx, psf_zyx):
+    # with the runtime-planned kernels everywhere (CLARITY_STATIC=0) the
+    # persistent launch's volumes equal their single solves bit for bit
+    # (emu_main checks), whatever order the queue hands out work in
+    r = syn.rng(3 + sum(img_zyx))
+    img = (r.random(img_zyx) * 100 + 1).astype(np.float32)
+    psf = syn.gaussian_psf(psf_zyx, 1.5, 1.2).astype(np.float32)
+    os.environ["CLARITY_STATIC"] = "0"
+    try:
+        a = run_emu(emu, tmp_path, "batchp", img, psf, 2)
+        os.environ["EMU_BLOCK_ORDER"] = "reverse"
+        b = run_emu(emu, tmp_path, "batchp", img, psf, 2)
+    finally:
+        os.environ.pop("CLARITY_STATIC", None)
+        os.environ.pop("EMU_BLOCK_ORDER", None)
+    assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("dims,chans", [((8, 6, 10), (16, 0, 16)), ((4, 6, 8), (16, 32, 48)),

@@ -155,3 +155,21 @@ def test_batched_workload_volumes(clarity_gpu, ref_cpu, oracle_lib):
     clarity_gpu.ml_device(di[0], dk[0], one, iters)
     torch.cuda.synchronize()
     assert torch.equal(one, outs[0])
+    # the persistent launch (all volumes' iterations through one work queue):
+    # against the reference and FP64 like the per-volume batch, within 1e-6
+    # of it, and a replay of its captured graph gives the same bits
+    pers = [torch.full_like(a, -1.0) for a in di]
+    clarity_gpu.ml_batch_device(di, dk, pers, iters, graph=True, persistent=True)
+    torch.cuda.synchronize()
+    first = [p.clone() for p in pers]
+    for i, (img, psf), a, b in zip(BATCH_IDS, cases, outs, pers):
+        got = b.cpu().numpy()
+        _check(f"batched_persistent_vol{i}_rl{iters}_{img.shape[2]}x{img.shape[1]}x"
+               f"{img.shape[0]}", got, _ref32(ref_cpu, oracle_lib, "rl", img, psf, iters),
+               _ref64(oracle_lib, "rl", img, psf, iters), TOL_ITER)
+        assert rel_l2(got, a.cpu().numpy()) <= 1e-6, i
+    clarity_gpu.ml_batch_device(di, dk, pers, iters, graph=True, persistent=True)
+    torch.cuda.synchronize()
+    for a, b in zip(first, pers):
+        assert torch.equal(a, b)
+    clarity_gpu.synchronize()
