@@ -15,6 +15,26 @@
 namespace clarity {
 
 // ------------------------------------------------------------------------
+// Index arithmetic by runtime divisors.  A pass's work items are numbered
+// f = threadIdx.x + k*blockDim.x and split into (line, block, i) by the
+// plan's extents; an integer division by a runtime value costs a long
+// instruction sequence per item.  DivR keeps d and 1/d (one float division
+// per pass): for 0 <= n < 2^22 the float quotient n*(1/d) is within a half
+// of n/d, so its truncation is off by at most one, which one compare fixes.
+struct DivR {
+  int d;
+  float r;
+};
+__device__ __forceinline__ DivR div_by(int d) { return DivR{d, 1.0f / (float)d}; }
+__device__ __forceinline__ int quot(int n, DivR D) {
+  int q = (int)((float)n * D.r);
+  const int rem = n - q * D.d;
+  if (rem >= D.d) ++q;
+  else if (rem < 0) --q;
+  return q;
+}
+
+// ------------------------------------------------------------------------
 // Shared-memory addressing of one x row in the XY kernels (padded so the
 // digit-reversed column reads of the r2c step are bank-conflict free).
 __device__ __forceinline__ int xpos(const VolPlan& P, int e) {
@@ -43,20 +63,24 @@ __device__ __forceinline__ void smem_pass(float2* sm, const VolPlan& P,
   const int per_line = nblk * span;  // = n / R
   const int total = nlines * per_line;
   const int twstep = n / len;
+  const DivR Dl0 = div_by(l0n), Dpl = div_by(per_line), Dsp = div_by(span);
   for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    int l, rem;
+    int l, rem, lq, lr;  // line l = lq*l0n + lr
     if (l0fast) {
-      const int l0 = f % l0n;
-      const int rest = f / l0n;
-      rem = rest % per_line;
-      l = (rest / per_line) * l0n + l0;
+      const int rest = quot(f, Dl0);
+      lr = f - rest * l0n;
+      lq = quot(rest, Dpl);
+      rem = rest - lq * per_line;
+      l = lq * l0n + lr;
     } else {
-      l = f / per_line;
+      l = quot(f, Dpl);
       rem = f - l * per_line;
+      lq = quot(l, Dl0);
+      lr = l - lq * l0n;
     }
-    const int b = rem / span;
+    const int b = quot(rem, Dsp);
     const int i = rem - b * span;
-    const int lb = (l / l0n) * s1 + (l % l0n) * s0;
+    const int lb = lq * s1 + lr * s0;
     const int e0 = b * len + i;
     float2 v[R];
 #pragma unroll
@@ -141,10 +165,11 @@ __device__ __forceinline__ void x_first_pass(float2* sm, const VolPlan& P,
   const int span = A.span[0];
   const int rows = P.G * P.Ay;
   const int total = rows * span;
+  const DivR Dsp = div_by(span), Day = div_by(P.Ay);
   for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    const int r = f / span;
+    const int r = quot(f, Dsp);
     const int i = f - r * span;
-    const int g = r / P.Ay, j = r - g * P.Ay;
+    const int g = quot(r, Day), j = r - g * P.Ay;
     const int y = y0base + g + P.By * j;
     float2 v[R];
 #pragma unroll
@@ -166,10 +191,11 @@ __device__ __forceinline__ void x_load_only(float2* sm, const VolPlan& P,
                                             const Pro& pro, int z, int y0base) {
   const int rows = P.G * P.Ay;
   const int total = rows * P.M;
+  const DivR Dm = div_by(P.M), Day = div_by(P.Ay);
   for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    const int r = f / P.M;
+    const int r = quot(f, Dm);
     const int m = f - r * P.M;
-    const int g = r / P.Ay, j = r - g * P.Ay;
+    const int g = quot(r, Day), j = r - g * P.Ay;
     const int y = y0base + g + P.By * j;
     sm[r * P.rowStride + xpos(P, m)] = pro.load_c(m, y, z);
   }
@@ -216,9 +242,10 @@ __device__ __forceinline__ void r2c_cols_forward(const float2* sm,
   const float2* twr = tw + P.tw_r2c_off;
   const float2* twny = tw + P.tw_ny_off;
   const int total = P.G * P.items;
+  const DivR Dg = div_by(P.G);
   for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    const int g = f % P.G;
-    const int it = f / P.G;
+    const int it = quot(f, Dg);
+    const int g = f - it * P.G;
     const int y0 = y0base + g;
     const float2* rows = sm + (g * AY) * P.rowStride;
     if (P.xmode == 1) {
@@ -303,9 +330,10 @@ __device__ __forceinline__ void c2r_cols_inverse(float2* sm, const VolPlan& P,
   const float2* twr = tw + P.tw_r2c_off;
   const float2* twny = tw + P.tw_ny_off;
   const int total = P.G * P.items;
+  const DivR Dg = div_by(P.G);
   for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    const int g = f % P.G;
-    const int it = f / P.G;
+    const int it = quot(f, Dg);
+    const int g = f - it * P.G;
     const int y0 = y0base + g;
     float2* rows = sm + (g * AY) * P.rowStride;
     if (P.xmode == 1) {
@@ -410,10 +438,11 @@ __device__ __forceinline__ void x_last_pass(float2* sm, const VolPlan& P,
   const int span = A.npass > 0 ? A.span[0] : 1;
   const int rows = P.G * P.Ay;
   const int total = rows * span;
+  const DivR Dsp = div_by(span), Day = div_by(P.Ay);
   for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    const int r = f / span;
+    const int r = quot(f, Dsp);
     const int i = f - r * span;
-    const int g = r / P.Ay, j = r - g * P.Ay;
+    const int g = quot(r, Day), j = r - g * P.Ay;
     const int y = y0base + g + P.By * j;
     float2* row = sm + r * P.rowStride;
     float2 v[R];
