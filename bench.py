@@ -678,6 +678,35 @@ def run_gpu_arm(args, rank, world):
         dist.destroy_process_group()
 
 
+def profile_case(which):
+    """A small case of one kernel family for ncu captures (see --profile-case)."""
+    import torch
+    from clarity_b200 import api, unet, synthetic as syn
+    api.load()
+    api.register()
+    if which == "conv":
+        g = torch.Generator(device="cuda").manual_seed(0)
+        for (D, H, W, c1, c2, co) in [(64, 256, 256, 16, 0, 16), (32, 128, 128, 32, 64, 32)]:
+            def rnd(*shape, s=1.0):
+                return ((torch.rand(shape, device="cuda", generator=g) - 0.5) * s).to(torch.bfloat16)
+            x1 = rnd(D, H, W, c1)
+            x2 = rnd(D // 2, H // 2, W // 2, c2) if c2 else None
+            w = rnd(co, 27, c1 + c2, s=0.1)
+            b = torch.zeros(co, device="cuda")
+            for _ in range(2):
+                unet.conv3(x1, w, co, bias=b, relu=True, x2=x2)
+    else:
+        cases = [syn.cfg2_volume(i)[:2] for i in (3, 5, 9, 12)]
+        di = [torch.from_numpy(a).cuda() for a, _ in cases]
+        dk = [torch.from_numpy(b).cuda() for _, b in cases]
+        outs = [torch.empty_like(a) for a in di]
+        api.ml_batch_device(di, dk, outs, 2, graph=False, persistent=True)
+    torch.cuda.synchronize()
+    api.synchronize()
+    api.unregister()
+    print(json.dumps({"profile_case": which, "ok": True}), flush=True)
+
+
 def main():
     global ITERS
     ap = argparse.ArgumentParser()
@@ -691,10 +720,19 @@ def main():
                          "for profiling captures)")
     ap.add_argument("--quick", action="store_true",
                     help="device leg only (no e2e, no CPU baseline): for ncu captures")
+    ap.add_argument("--profile-case", choices=["conv", "batch"], default=None,
+                    help="run one small case for an ncu capture and exit: 'conv' two "
+                         "launches each of the learned-start network's 16->16 layer at "
+                         "64x256x256 and its 96->32 decoder layer at 32x128x128; 'batch' the "
+                         "persistent batched RL launch over four batched-workload volumes, "
+                         "two iterations")
     args = ap.parse_args()
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
     ITERS = args.iters
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:
