@@ -91,53 +91,39 @@ __device__ __forceinline__ void per_task_two_phase(const A& a, const B& b) {
 #endif
 }
 
-// Runs f(row, k, pa, pb, w) for the tile rows j < L of every line and every
-// pair 0 < k < M/2 of slots pa = slot(k), pb = slot(M - k), w = twr[k] (rows
-// j >= L are known zeros or not needed).  With KP (the power of two >= the
-// pair count) dividing the block, each thread keeps one k for all its rows,
-// so the slots and the twiddle are computed once.
-template <class SH, class F>
-__device__ __forceinline__ void for_each_pair(float2* buf, const float2* __restrict__ twr,
-                                              const F& f, int L = XyTma<SH>::AY) {
-  using X = XyTma<SH>;
-  using T = typename X::T;
-  constexpr int M = X::M, NP = M / 2 - 1, AY = X::AY;
-  const int NR = X::TG * L;  // rows visited
-  // visited row rv -> tile row g * AY + j, j < L
-  auto row_of = [&](int rv) {
-    const int g = rv / L;
-    return g * AY + (rv - g * L);
-  };
-  constexpr int KP = NP < 2 ? 1 : (1 << (32 - __builtin_clz(NP - 1)));
-  constexpr int TH = SH::THREADS;
+// As per_task_two_phase, and b also gets other(j): row j of the partner
+// task c ^ 1 (the column M - kx of the pair), from a warp shuffle on the GPU
+// (every task's lane pair shares a warp: TASKS is a multiple of 32 and
+// tasks are threads) or from the array in the CPU emulation.  other(j) must
+// be called by every thread, in uniform control flow.
+template <int TASKS, int AY, class A, class B>
+__device__ __forceinline__ void per_task_two_phase_pairs(const A& a, const B& b) {
+  static_assert(TASKS % 32 == 0, "a task's pair partner must be in its warp");
 #ifndef CLARITY_HOST_EMULATION
-  constexpr bool kFixedK = KP <= TH && TH % KP == 0;
+  float2 v[AY];
+  const int c = threadIdx.x;
+  if (c < TASKS) a(c, v);
+  __syncthreads();
+  auto other = [&](int j) {
+    return make_float2(__shfl_xor_sync(0xffffffffu, v[j].x, 1),
+                       __shfl_xor_sync(0xffffffffu, v[j].y, 1));
+  };
+  if (c < TASKS) b(c, v, other);
 #else
-  constexpr bool kFixedK = false;  // one thread per block: the strided loop
-#endif
-  if constexpr (kFixedK) {
-    constexpr int RSTEP = TH / KP;
-    const int k = 1 + (int)threadIdx.x % KP;
-    if (k <= NP) {
-      const int pa = xp<T>(xrev<T>(k)), pb = xp<T>(xrev<T>(M - k));
-      const float2 w = __ldg(&twr[k]);
-#pragma unroll 2
-      for (int rv = (int)threadIdx.x / KP; rv < NR; rv += RSTEP)
-        f(buf + row_off<T>(row_of(rv)), pa, pb, w);
-    }
-  } else {
-#pragma unroll 1
-    for (int q = threadIdx.x; q < NR * NP; q += CLARITY_BLOCK_STRIDE(TH)) {
-      const int k = 1 + q % NP;
-      const int r = row_of(q / NP);
-      f(buf + row_off<T>(r), xp<T>(xrev<T>(k)), xp<T>(xrev<T>(M - k)), __ldg(&twr[k]));
-    }
+  std::vector<float2> regs((size_t)TASKS * AY);
+  for (int c = 0; c < TASKS; ++c) a(c, &regs[(size_t)c * AY]);
+  for (int c = 0; c < TASKS; ++c) {
+    const float2* o = &regs[(size_t)(c ^ 1) * AY];
+    auto other = [o](int j) { return o[j]; };
+    b(c, &regs[(size_t)c * AY], other);
   }
+#endif
 }
 
 // Inverse column step: box (natural kx) -> x rows (digit-reversed slots),
-// then the c2r pair combine of slots k and M - k.  Only rows j < L of each
-// line are written (the later steps read no others).
+// with the c2r pair combine of slots k and M - k done as the rows are
+// written (the pair's two columns are held by two lanes of one warp).  Only
+// rows j < L of each line are written (the later steps read no others).
 template <class SH>
 __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
                                                  const float2* __restrict__ twr,
@@ -168,42 +154,41 @@ __device__ __forceinline__ void cols_inverse_tma(float2* buf, int y0base,
     dft<AY, +1>(v);
   };
   // after the barrier every column is held: the box may be overwritten
-  auto store = [&](int c, const float2* v) {
+  auto store = [&](int c, const float2* v, const auto& other) {
     const int g = c / M, cc = c - g * M;
     float2* rows = buf + g * T::GSTRIDE;
-    if (cc == 0) {
-      const int p0 = xp<T>(0);
+    // pair (k, M - k), 0 < k < M/2: the even task holds X[k], the odd X[M-k]
+    const bool pair = cc >= 2, odd = (cc & 1) != 0;
+    const int p = cc == 0 ? xp<T>(0)
+                          : xp<T>(xrev<T>(cc == 1 ? M / 2 : task_kx(cc, M)));
+    const float2 w = pair ? __ldg(&twr[cc >> 1]) : make_float2(1.f, 0.f);
 #pragma unroll
-      for (int j = 0; j < AY; ++j)
-        if (j < L) rows[j * RS + p0] = make_float2(v[j].x + v[j].y, v[j].x - v[j].y);
-    } else if (cc == 1) {
-      const int ph = xp<T>(xrev<T>(M / 2));
-#pragma unroll
-      for (int j = 0; j < AY; ++j)
-        if (j < L) rows[j * RS + ph] = make_float2(2.f * v[j].x, -2.f * v[j].y);
-    } else {
-      const int p = xp<T>(xrev<T>(task_kx(cc, M)));
-#pragma unroll
-      for (int j = 0; j < AY; ++j)
-        if (j < L) rows[j * RS + p] = v[j];
+    for (int j = 0; j < AY; ++j) {
+      if (j >= L) continue;  // L is the same for every thread
+      const float2 ov = other(j);
+      if (cc == 0) {
+        rows[j * RS + p] = make_float2(v[j].x + v[j].y, v[j].x - v[j].y);
+      } else if (cc == 1) {
+        rows[j * RS + p] = make_float2(2.f * v[j].x, -2.f * v[j].y);
+      } else {
+        const float2 xa = odd ? ov : v[j];
+        const float2 b = conjf2(odd ? v[j] : ov);
+        const float2 e = cadd(xa, b);
+        const float2 o = cmulc(csub(xa, b), w);
+        rows[j * RS + p] = odd ? make_float2(e.x + o.y, -e.y + o.x)
+                               : make_float2(e.x - o.y, e.y + o.x);
+      }
     }
   };
-  per_task_two_phase<X::TASKS, AY>(load, store);
-  __syncthreads();
-  for_each_pair<SH>(buf, twr, [](float2* row, int pa, int pb, float2 w) {
-    const float2 xa = row[pa];
-    const float2 b = conjf2(row[pb]);
-    const float2 e = cadd(xa, b);
-    const float2 o = cmulc(csub(xa, b), w);
-    row[pa] = make_float2(e.x - o.y, e.y + o.x);
-    row[pb] = make_float2(e.x + o.y, -e.y + o.x);
-  }, L);
+  per_task_two_phase_pairs<X::TASKS, AY>(load, store);
   __syncthreads();
 }
 
 // Forward column step: x rows (digit-reversed slots) -> box (natural kx),
-// every kx < KG*W written (slots beyond M are zero).  Rows j >= L of each
-// line hold zeros: the pair split leaves them so and skips them.
+// every kx < KG*W written (slots beyond M are zero).  The r2c split of
+// slots k and M - k happens as the columns are read: both tasks of a pair
+// read both slots and each keeps its own half.  Rows j >= L of each line
+// hold zeros, which the split maps to zeros.
 template <class SH>
 __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
                                                  const float2* __restrict__ twr,
@@ -212,18 +197,7 @@ __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
   using X = XyTma<SH>;
   using T = typename X::T;
   constexpr int M = X::M, AY = X::AY, RS = T::ROWSTRIDE;
-  // r2c split of slots k and M - k, in place
-  for_each_pair<SH>(buf, twr, [](float2* row, int pa, int pb, float2 w) {
-    const float2 a = row[pa];
-    const float2 b = conjf2(row[pb]);
-    const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
-    const float2 d = csub(a, b);
-    const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
-    const float2 wo = cmul(w, o);
-    row[pa] = cadd(e, wo);
-    row[pb] = conjf2(csub(e, wo));
-  }, L);
-  __syncthreads();
+  (void)L;
   auto load = [&](int c, float2* v) {
     const int g = c / M, cc = c - g * M;
     const float2* rows = buf + g * T::GSTRIDE;
@@ -252,9 +226,21 @@ __device__ __forceinline__ void cols_forward_tma(float2* buf, int y0base,
       for (int j = 0; j < AY; ++j) v[j] = conjf2(rows[j * RS + ph]);
       dft<AY, -1>(v);
     } else {
-      const int p = xp<T>(xrev<T>(task_kx(cc, M)));
+      // pair (k, M - k): the even task keeps X[k], the odd X[M - k]
+      const int k = cc >> 1;
+      const bool odd = (cc & 1) != 0;
+      const int pa = xp<T>(xrev<T>(k)), pb = xp<T>(xrev<T>(M - k));
+      const float2 w = __ldg(&twr[k]);
 #pragma unroll
-      for (int j = 0; j < AY; ++j) v[j] = rows[j * RS + p];
+      for (int j = 0; j < AY; ++j) {
+        const float2 a = rows[j * RS + pa];
+        const float2 b = conjf2(rows[j * RS + pb]);
+        const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
+        const float2 d = csub(a, b);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        const float2 wo = cmul(w, o);
+        v[j] = odd ? conjf2(csub(e, wo)) : cadd(e, wo);
+      }
       dft<AY, -1>(v);
     }
   };
