@@ -25,6 +25,7 @@
 #include "plan.hpp"
 
 namespace clarity {
+CLARITY_EXTERN_PASS_KERNELS
 namespace {
 
 // 32 MiB: the plan tables, the OTF and the work spectrum.  The limit is in

@@ -629,7 +629,12 @@ __device__ __forceinline__ void z_body(float2* sm, const VolPlan& P, const Mod& 
 }
 
 // ------------------------------------------------------------------------
-// Kernels: one body per block.
+// Kernels: one body per block.  Each instance is compiled in exactly one
+// translation unit (the kern_*.cu file of its family, which defines it
+// explicitly); other units name it through CLARITY_EXTERN_PASS_KERNELS.  Two
+// compiled copies of one kernel (say one with scalar and one with paired
+// FP32 adds) would both register for the same launch and the runtime would
+// run either, so results could differ between processes.
 template <class Pro>
 __global__ void __launch_bounds__(256, 2)
     k_xy_forward(const VolPlan P, const Pro pro, float2* CLARITY_RESTRICT S,
@@ -661,5 +666,19 @@ __global__ void __launch_bounds__(256, 2)
   CLARITY_DYN_SMEM(float2, sm);
   z_body(sm, P, mod, Sin, Sout, tw, (int)blockIdx.x);
 }
+
+// The generic pass kernels the no-allocation convolution (noalloc.cu)
+// launches, defined in kern_xy_fwd.cu, kern_z.cu and kern_xy_inv.cu.
+#define CLARITY_EXTERN_PASS_KERNELS                                                           \
+  extern template __global__ void k_xy_forward<ProPadded>(const VolPlan, const ProPadded,     \
+                                                          float2*, const float2*, const int*); \
+  extern template __global__ void k_xy_forward<ProImage>(const VolPlan, const ProImage,       \
+                                                         float2*, const float2*, const int*);  \
+  extern template __global__ void k_z<ModForward>(const VolPlan, const ModForward,            \
+                                                  const float2*, float2*, const float2*);      \
+  extern template __global__ void k_z<ModOTF>(const VolPlan, const ModOTF, const float2*,     \
+                                              float2*, const float2*);                         \
+  extern template __global__ void k_xy_inverse<EpiClip>(const VolPlan, EpiClip, const float2*, \
+                                                        const float2*, const int*);
 
 }  // namespace clarity

@@ -157,7 +157,9 @@ def test_batched_workload_volumes(clarity_gpu, ref_cpu, oracle_lib):
     assert torch.equal(one, outs[0])
     # the persistent launch (all volumes' iterations through one work queue):
     # against the reference and FP64 like the per-volume batch, within 1e-6
-    # of it, and a replay of its captured graph gives the same bits
+    # of it (its z bodies use paired FP32 adds, the per-volume z kernels
+    # scalar adds and FMAs), and a replay of its captured graph gives the
+    # same bits
     pers = [torch.full_like(a, -1.0) for a in di]
     clarity_gpu.ml_batch_device(di, dk, pers, iters, graph=True, persistent=True)
     torch.cuda.synchronize()
