@@ -383,21 +383,35 @@ def cached_reference(name, inputs):
     return np.load(path) if os.path.exists(path) else None
 
 
+SUB = 16  # sample stride of the kept precision-form references
+
+
 def precision_forms(api, torch, stream, iters=100):
     """The precision workload: RL for `iters` iterations on the 512x512x128
     volume (work box 1024x1024x256) with the FP32 register FFT and with the
     first radix-16 z stage as split hi+lo FP16 / BF16 tensor-core GEMMs; time
     (CUDA events) and the error against the FP64 oracle where its output has
-    been computed (tests/golden/_large)."""
+    been computed (tests/golden/_large).  The full outputs (134 MB each) may
+    be kept as every SUB-th voxel (name suffix "-sub"): the errors are then
+    taken over that sample."""
     from clarity_b200 import synthetic as syn
     img, psf, _ = syn.cfg3()
     r64 = cached_reference(f"rl{iters}-f64", [img, psf])
     r32 = cached_reference(f"rl{iters}-ref32", [img, psf])
+    pick = lambda a: a  # noqa: E731 (the whole volume)
+    if r64 is None or r32 is None:
+        r64 = cached_reference(f"rl{iters}-f64-sub", [img, psf])
+        r32 = cached_reference(f"rl{iters}-ref32-sub", [img, psf])
+        pick = lambda a: np.ascontiguousarray(a).ravel()[::SUB]  # noqa: E731
+    if r64 is not None:
+        r64 = r64.astype(np.float64)
     di, dk = torch.from_numpy(img).cuda(), torch.from_numpy(psf).cuda()
     out = torch.empty_like(di)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     res = {"workload": f"RL 512x512x128 fp32 (work box 1024x1024x256), {iters} iterations",
-           "fp64_reference": r64 is not None}
+           "fp64_reference": r64 is not None,
+           "error_sample": None if r64 is None else (
+               "every voxel" if r64.size == img.size else f"every {SUB}th voxel")}
     if r64 is not None and r32 is not None:
         res["reference_build_rel_l2_vs_fp64"] = float(np.linalg.norm(
             (r32.astype(np.float64) - r64).ravel()) / np.linalg.norm(r64.ravel()))
@@ -415,7 +429,7 @@ def precision_forms(api, torch, stream, iters=100):
         ms = e0.elapsed_time(e1)
         row = {"ms": ms, "value": img.size * iters / (ms / 1e3) / 1e9, "unit": "Gvoxel-iter/s"}
         if r64 is not None:
-            got = out.cpu().numpy().astype(np.float64)
+            got = pick(out.cpu().numpy()).astype(np.float64)
             row["rel_l2_vs_fp64"] = float(np.linalg.norm((got - r64).ravel()) /
                                           np.linalg.norm(r64.ravel()))
             row["max_abs_vs_fp64"] = float(np.abs(got - r64).max())
