@@ -213,7 +213,9 @@ def max_over_ranks(value, dist, device):
 def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=60):
     """The second metric: device time until I-div(g, h*u) is within 1% of
     plain RL's value after `plain_iters` iterations, for plain RL and for the
-    chosen form (Biggs-Andrews accelerated RL), on the same GPU and inputs.
+    chosen form (the faster of Biggs-Andrews accelerated RL and, where its
+    trained weights are present, the learned start), on the same GPU and
+    inputs.
     The I-divergence of every plain iterate comes from the trace the ratio
     pass accumulates; the chosen form's iteration count is the smallest whose
     result meets the target (its own traced final I-divergence)."""
@@ -285,6 +287,16 @@ def time_to_target(api, torch, img_d, psf_d, stream, plain_iters=200, max_accel=
                 ls["speedup"] = res["plain"]["ms"] / ls["ms"]
             res[tag] = ls
         res["network"] = network_layers(torch, net)
+    # the chosen form is the fastest one that meets the target: accelerated
+    # RL needs no trained weights; the learned start (whose result the tests
+    # hold to 1e-3 of the FP64 oracle) is faster where its weights are present
+    res["accelerated"] = dict(res["chosen"])
+    best = min((f for f in ("learned_start", "learned_start_accel") if "ms" in res.get(f, {})),
+               key=lambda f: res[f]["ms"], default=None)
+    if best and res[best]["ms"] < res["chosen"].get("ms", float("inf")):
+        res["chosen"] = dict(res[best], iterations=res[best]["pre_iterations"] +
+                             res[best]["resumed_iterations"])
+        res["speedup"] = res[best]["speedup"]
     return res
 
 
