@@ -176,7 +176,7 @@ __device__ __forceinline__ void run_item(float2* sm, const VolPlan& P, const Vol
   }
 }
 
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_GEN_MINB)
     k_rl_batch(const Vol* vols, const VolSet* sets, const long long* pre, const Queue q) {
   CLARITY_DYN_SMEM(float2, sm);
   __shared__ int s_stop, s_k, s_kind, s_vol;

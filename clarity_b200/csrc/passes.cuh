@@ -635,8 +635,13 @@ __device__ __forceinline__ void z_body(float2* sm, const VolPlan& P, const Mod& 
 // compiled copies of one kernel (say one with scalar and one with paired
 // FP32 adds) would both register for the same launch and the runtime would
 // run either, so results could differ between processes.
+// Blocks per SM the runtime-planned kernels' register budget is sized for.
+#ifndef CLARITY_GEN_MINB
+#define CLARITY_GEN_MINB 2
+#endif
+
 template <class Pro>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_GEN_MINB)
     k_xy_forward(const VolPlan P, const Pro pro, float2* CLARITY_RESTRICT S,
                  const float2* CLARITY_RESTRICT tw, const int* CLARITY_RESTRICT xrev) {
   CLARITY_DYN_SMEM(float2, sm);
@@ -644,7 +649,7 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <class Epi>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_GEN_MINB)
     k_xy_inverse(const VolPlan P, Epi epi, const float2* CLARITY_RESTRICT S,
                  const float2* CLARITY_RESTRICT tw, const int* CLARITY_RESTRICT xrev) {
   CLARITY_DYN_SMEM(float2, sm);
@@ -652,7 +657,7 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <class Mid>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_GEN_MINB)
     k_xy_inv_fwd(const VolPlan P, Mid mid, float2* CLARITY_RESTRICT S,
                  const float2* CLARITY_RESTRICT tw, const int* CLARITY_RESTRICT xrev) {
   CLARITY_DYN_SMEM(float2, sm);
@@ -660,7 +665,7 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 template <class Mod>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, CLARITY_GEN_MINB)
     k_z(const VolPlan P, const Mod mod, const float2* CLARITY_RESTRICT Sin,
         float2* CLARITY_RESTRICT Sout, const float2* CLARITY_RESTRICT tw) {
   CLARITY_DYN_SMEM(float2, sm);

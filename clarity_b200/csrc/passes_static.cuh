@@ -38,8 +38,12 @@ constexpr int ctz_c(int v) {
   return c;
 }
 
-// Even nx only (half-length complex rows).
-template <class XR, int AY_, class YR, class ZR, int G_, int W_>
+// Even nx only (half-length complex rows).  T_ threads per block: 256 where
+// several blocks fit an SM; the boxes whose XY and z tiles take most of an
+// SM's shared memory (one block per SM) use more threads, so the SM still
+// holds enough warps to hide shared-memory and HBM latency.  TZ_: the same
+// for the FP32 z kernel (launched as ZThreads<SH>, the shape with TZ_ threads).
+template <class XR, int AY_, class YR, class ZR, int G_, int W_, int T_ = 256, int TZ_ = T_>
 struct Shape {
   using X = XR;
   using Y = YR;
@@ -58,7 +62,12 @@ struct Shape {
   static constexpr int ITEMS = (M % 2 == 0) ? (M / 2 > 1 ? M / 2 : 1) : (M + 1) / 2;
   static constexpr int BW = BY * W;
   static constexpr int TILE = NZ * BW;
-  static constexpr int THREADS = 256;
+  static constexpr int THREADS = T_;
+  static constexpr int Z_THREADS = TZ_;
+  static_assert(T_ % 32 == 0 && T_ >= 256 && T_ <= 1024, "whole warps, 256..1024 threads");
+  // blocks per SM the register budget is sized for (__launch_bounds__)
+  static constexpr int XY_MINB = T_ == 256 ? CLARITY_XY_MINBLOCKS : 1;
+  static constexpr int Z_MINB = T_ == 256 ? 2 : 1;
   static constexpr int XY_SMEM = G * GSTRIDE * 8;
   static constexpr int Z_SMEM = TILE * 8;
   static constexpr int NGROUPS = BY / G;
@@ -71,6 +80,11 @@ struct Shape {
   static constexpr int Z2_TILE_BYTES = NZ * ZS * 8;
   static constexpr int Z2_SMEM = Z2_TILE_BYTES + NZ * 8;
 };
+
+// Shape SH with TZ_ threads for every kernel: the FP32 z kernel's launch shape.
+template <class SH>
+using ZThreads = Shape<typename SH::X, SH::AY, typename SH::Y, typename SH::Z, SH::G, SH::W,
+                       SH::Z_THREADS, SH::Z_THREADS>;
 
 template <class SH>
 __device__ __forceinline__ int xp(int e) {
@@ -538,7 +552,7 @@ struct Tables {
 
 // ----------------------------------------------------------------- kernels
 template <class SH, class Pro>
-__global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
+__global__ void __launch_bounds__(SH::THREADS, SH::XY_MINB)
     ks_xy_forward(const Pro pro, float2* __restrict__ S, const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
@@ -562,7 +576,7 @@ __device__ __forceinline__ void prefetch_tile_rows(const Epi& epi, int z, int y0
 }
 
 template <class SH, class Epi>
-__global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
+__global__ void __launch_bounds__(SH::THREADS, SH::XY_MINB)
     ks_xy_inverse(Epi epi, const float2* __restrict__ S, const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
@@ -576,7 +590,7 @@ __global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
 }
 
 template <class SH, class Mid>
-__global__ void __launch_bounds__(256, CLARITY_XY_MINBLOCKS)
+__global__ void __launch_bounds__(SH::THREADS, SH::XY_MINB)
     ks_xy_inv_fwd(Mid mid, float2* __restrict__ S, const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
   const int z = blockIdx.x / SH::NGROUPS;
@@ -634,7 +648,7 @@ constexpr bool kTcZ = SH::Z::radix(0) == 16 && SH::Z::npass >= 2 && SH::BW % 8 =
                       !SH::Y_PER_LINE;
 
 template <class SH, class Mod, int PREC = kDftF32>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(SH::THREADS, SH::Z_MINB)
     ks_z(const Mod mod, const float2* __restrict__ Sin, float2* __restrict__ Sout,
          const Tables T) {
   CLARITY_DYN_SMEM(float2, sm);
@@ -764,7 +778,7 @@ __device__ __forceinline__ void z2_last(float2* sm, const Mod& mod, unsigned gba
 }
 
 template <class SH, class Mod>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(SH::THREADS, SH::Z_MINB)
     ks_z2(const Mod mod, const float2* __restrict__ Sin, float2* __restrict__ Sout,
           const Tables T) {
   CLARITY_PDL_WAIT();  // the previous kernel's output is complete and visible

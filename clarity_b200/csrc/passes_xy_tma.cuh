@@ -52,9 +52,11 @@ struct XyTma {
   static constexpr bool TW_SMEM = 3 * (SMEM + TW_F2 * 8 + 2048 + 1024) <= 228 * 1024;
   static constexpr int THREADS = SH::THREADS;
   static constexpr int BLOCKS = SH::NZ * (SH::BY / TG);
-  // usable when the tile fits three blocks per SM, every column task has a
-  // thread, the rows are whole 16-byte runs and the box is a legal TMA box
-  static constexpr bool OK = SMEM <= 72 * 1024 && TASKS <= THREADS && M % 2 == 0 && M >= 4 &&
+  // usable when the tile fits three 256-thread blocks per SM, every column
+  // task has a thread, the rows are whole 16-byte runs and the box is a legal
+  // TMA box
+  static constexpr bool OK = SMEM <= 72 * 1024 && THREADS == 256 && TASKS <= THREADS &&
+                             M % 2 == 0 && M >= 4 &&
                              AY % 2 == 0 &&
                              NX % 4 == 0 && SH::BY % TG == 0 && KG <= 256 && AY <= 256 &&
                              (BOXW * 8) % 16 == 0;

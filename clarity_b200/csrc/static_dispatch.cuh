@@ -17,7 +17,18 @@ namespace clarity {
 
 using ShapeW512 = st::Shape<st::Rad<16, 16>, 16, st::Rad<8, 4>, st::Rad<16, 8>, 2, 2>;
 using ShapeW128 = st::Shape<st::Rad<8, 8>, 16, st::Rad<8>, st::Rad<8, 8>, 1, 4>;
-using ShapeW1024 = st::Shape<st::Rad<8, 8, 8>, 16, st::Rad<8, 8>, st::Rad<16, 16>, 2, 1>;
+// The 1024x1024x256 box's XY and z tiles (133 and 128 KB) leave room for one
+// block per SM, so its XY blocks run CLARITY_W1024_THREADS threads and its
+// FP32 z blocks CLARITY_W1024_Z_THREADS (both measured against 256; more XY
+// threads spill registers).  The tensor-core z form keeps the XY count.
+#ifndef CLARITY_W1024_THREADS
+#define CLARITY_W1024_THREADS 512
+#endif
+#ifndef CLARITY_W1024_Z_THREADS
+#define CLARITY_W1024_Z_THREADS 1024
+#endif
+using ShapeW1024 = st::Shape<st::Rad<8, 8, 8>, 16, st::Rad<8, 8>, st::Rad<16, 16>, 2, 1,
+                             CLARITY_W1024_THREADS, CLARITY_W1024_Z_THREADS>;
 using ShapeW64 = st::Shape<st::Rad<8, 4>, 16, st::Rad<4>, st::Rad<8, 4>, 4, 1>;
 
 // The 512x512x128 box keeps its TMA XY pass with shared-memory twiddles and
@@ -129,17 +140,19 @@ inline bool try_static(const PlanEntry& pe, cudaStream_t st, const F& fn, float2
                                                                                      Sa, T);
       note_launch_end(KK_Z, st);
     } else {
-      auto k = st::ks_z<SH, F>;
+      auto k = st::ks_z<st::ZThreads<SH>, F>;
+      int threads = SH::Z_THREADS;
       if constexpr (st::kTcZ<SH> && !F::forward_only) {
         // the precision form: tensor-core first z stage (the OTF stays FP32)
         const int prec = dft_precision();
         if (prec == st::kDftF16Split) k = st::ks_z<SH, F, st::kDftF16Split>;
         if (prec == st::kDftBF16Split) k = st::ks_z<SH, F, st::kDftBF16Split>;
+        if (prec != st::kDftF32) threads = SH::THREADS;
       }
       *err = allow_smem_st(k, SH::Z_SMEM);
       if (*err != cudaSuccess) return true;
       note_launch_begin(KK_Z, st);
-      CLARITY_LAUNCH(k, pe.P.z_blocks, SH::THREADS, SH::Z_SMEM, st)(fn, Sb, Sa, T);
+      CLARITY_LAUNCH(k, pe.P.z_blocks, threads, SH::Z_SMEM, st)(fn, Sb, Sa, T);
       note_launch_end(KK_Z, st);
     }
   } else if constexpr (KIND == 2) {
