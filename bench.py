@@ -518,10 +518,16 @@ def other_configs(api, torch, stream, n_batch=64, batch_iters=30, cfg3_iters=10)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    # the survey's per-iteration bytes (4R + 10C) of the work box, as the
+    # headline's survey_frac
+    fb = family_bytes(tuple(2 * d for d in img.shape), img.size, psf.size, cfg3_iters)
+    large_gbps = fb["per_iteration_survey"] * cfg3_iters / (ms / 1e3) / 1e9
     res["large_rl"] = {"workload": f"RL 512x512x128 fp32 (work box 1024x1024x256), {cfg3_iters} "
                                    "iterations, FP32 SIMT FFT", "ms": ms,
                        "value": img.size * cfg3_iters / (ms / 1e3) / 1e9,
-                       "unit": "Gvoxel-iter/s"}
+                       "unit": "Gvoxel-iter/s",
+                       "survey_bytes_per_iteration": fb["per_iteration_survey"],
+                       "survey_GBps": large_gbps, "survey_frac": large_gbps / peak}
     del di, dk, out
     res["precision_forms"] = precision_forms(api, torch, stream)
     return res
